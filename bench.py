@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""Benchmark of the 2D pseudo-spectral vorticity DNS step on B200.
+
+Workload: plain DNS at N=4096 (6144 x 6144 dealiased physical grid), Re=1e5, K0=4, CFL=0.1,
+ADAPT_VISC=0, diagnostics (NEXTDT + OM2PHYS + display sigma) every UPDATE=100 steps as in the
+reference's mem_cuda loop.  A "step" is one time step (row pass + column pass); the timed K
+steps include their diagnostic steps, like the reference's "Steady FPS".  Initial field: seeded
+random-phase k^4 exp(-2(k/K0)^2) spectrum, E = 1/2 (synthetic).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--gpus N > 1 runs under torchrun, one independent replica per GPU (the solver does not shard;
+value = all replicas' steps / max-over-ranks device time).  --impl reference runs the
+reference's own cuFFT build (oracle/_ref/mem_cuda, compiled from its unmodified sources) on the
+same arguments and reports its Steady FPS; when that binary is absent it times the FP64 oracle.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOAD = dict(N=4096, Re=1.0e5, K0=4.0, CFL=0.1, UPDATE=100, ADAPT_VISC=0, seed=0)
+METRIC = "steps/s (2D vorticity DNS time step, N=4096, 6144^2 padded grid)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=WORKLOAD["N"])
+    ap.add_argument("--cpu-steps", type=int, default=3, help="FP64 oracle steps for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------
+# clock sampling during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# the run loop of the reference (cuda/mem_cuda.cu:1848-1897), through the C ABI
+# ------------------------------------------------------------------------------------------
+def advance(s, it_to, update, steps_total, counts, history=False):
+    """Advance a Solver to step it_to with the reference's diagnostic cadence."""
+    hist = []
+    while True:
+        it = s.scalars()["it"]
+        if it >= it_to:
+            break
+        nxt = it_to
+        if it < 1:
+            nxt = 1
+        else:
+            nxt = min(it_to, (it // update + 1) * update)
+        n = nxt - it
+        r = s.step(n, history=history)
+        if history:
+            hist.append(r)
+        counts["kernels"] += 2 * n + (n + 127) // 128
+        if nxt == 1 or nxt % update == 0 or nxt == steps_total:
+            s.next_dt()
+            s.om2phys()
+            s.display_sigma(2)
+            counts["kernels"] += 5
+    return hist
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import optimizec_b200 as P
+
+    N, K, W = args.n, args.steps, args.warmup
+    up = WORKLOAD["UPDATE"]
+    steps_total = W + K
+    torch.cuda.set_device(local_rank)
+    s = P.Solver(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"], device=local_rank)
+    s.init_k4(WORKLOAD["seed"] + rank)
+    s.next_dt()
+    counts = {"kernels": 0}
+    advance(s, W, up, steps_total, counts)
+    s.sync()
+    stream = torch.cuda.ExternalStream(s.stream(), device=local_rank)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    counts = {"kernels": 0}
+    ev0.record(stream)
+    advance(s, W + K, up, steps_total, counts)
+    ev1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    ms_max = float(t.item())
+    value = world * K / (ms_max / 1e3)
+
+    # per-kernel device time (CUDA events around each launch, on the solver's stream)
+    s.phase_timing(True)
+    s.step(20)
+    ph_ms, ph_n = s.phase_report()
+    s.phase_timing(False)
+    rows_ms = ph_ms[0] / max(ph_n[0], 1)
+    cols_ms = ph_ms[1] / max(ph_n[1], 1)
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(s, P, N, K, W, up, local_rank, world)
+    s.close()
+    return dict(value=value, ms=ms_max, K=K, W=W, N=N, kernels=counts["kernels"], clocks=ck,
+                rows_ms=rows_ms, cols_ms=cols_ms, e2e=e2e)
+
+
+def run_e2e(s_old, P, N, K, W, up, local_rank, world):
+    """Same metric through the public API with host buffers: pinned host state -> device,
+    K steps (per-step FP64 energy/enstrophy back to the host), final state -> host."""
+    import numpy as np
+    import torch
+
+    H = N // 2
+    om = P.k4_spectrum(N, WORKLOAD["K0"], WORKLOAD["seed"])
+    pin_om = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy()
+    pin_fn = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy()
+    pin_om[...] = om.view(np.float32).reshape(N, H, 2)
+    pin_fn[...] = 0.0
+    s = P.Solver(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"], device=local_rank)
+    # warm the graphs of this state
+    s.init_vorticity(pin_om.view(np.complex64).reshape(N, H), pin_fn.view(np.complex64).reshape(N, H))
+    s.next_dt()
+    advance(s, W, up, W + K, {"kernels": 0})
+    s.sync()
+    out_om = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    s.init_vorticity(pin_om.view(np.complex64).reshape(N, H), pin_fn.view(np.complex64).reshape(N, H))
+    s.next_dt()
+    advance(s, K, up, K, {"kernels": 0}, history=True)
+    res_om = s.om2()
+    res_fn = s.fnm1()
+    out_om[...] = res_om.view(np.float32).reshape(N, H, 2)
+    t1 = time.perf_counter()
+    sec = t1 - t0
+    t = torch.tensor([sec], device=f"cuda:{local_rank}", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    sec = float(t.item())
+    s.close()
+    state_bytes = 2 * N * H * 8
+    return {"value": world * K / sec, "unit": "steps/s",
+            "h2d_bytes_per_step": (state_bytes + 16 * K) / K,
+            "d2h_bytes_per_step": (state_bytes + 16 * K) / K,
+            "what": "host om2+fnm1 -> device, K steps with per-step E/Z to host, om2+fnm1 -> host"}
+
+
+def cpu_baseline(args):
+    from oracle import oracle as O
+    N = args.n
+    o = O.Oracle(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"])
+    o.init_om2(O.k4_spectrum(N, WORKLOAD["K0"], WORKLOAD["seed"]))
+    k = max(1, args.cpu_steps)
+    t0 = time.perf_counter()
+    o.run(k, 1000000, 1000000, want_diag=False)
+    sec = time.perf_counter() - t0
+    o.close()
+    return {"value": k / sec, "unit": "steps/s", "cores": O.threads(), "kind": "port",
+            "sample": f"{k} time steps of the FP64 oracle (oracle/dns2d_oracle.c, OpenMP) at N={N}, "
+                      f"{sec:.1f} s"}
+
+
+def ncu_traffic():
+    p = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def main_ours(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device(f"cuda:{local_rank}"))
+    r = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    N = r["N"]
+    peak, peak_kind = measured_peaks()
+    bytes_rows = 24 * N * N   # read U,W (12 N^2), write D,E (12 N^2)
+    bytes_cols = 40 * N * N   # read D,E + om2,fnm1 (20 N^2), write U,W + om2,fnm1 (20 N^2)
+    if r["rows_ms"] >= r["cols_ms"]:
+        name, b, ms = "k_rows_step", bytes_rows, r["rows_ms"]
+    else:
+        name, b, ms = "k_cols_step", bytes_cols, r["cols_ms"]
+    achieved = b / (ms / 1e3) / 1e9
+    tr = ncu_traffic().get(f"{name}<{N}>")
+    steps_s = r["value"] / max(1, int(os.environ.get("WORLD_SIZE", "1")))
+    line = {
+        "metric": METRIC,
+        "value": round(r["value"], 3),
+        "unit": "steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": r["K"],
+        "warmup": r["W"],
+        "ms_per_step": round(r["ms"] / r["K"], 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"plain DNS N={N} (6144^2 padded grid), Re=1e5, K0=4, CFL=0.1, "
+                               f"ADAPT_VISC=0, UPDATE={WORKLOAD['UPDATE']}, k^4 exp(-2(k/K0)^2) IC",
+                   "N": N, "padded_grid": 3 * N // 2, "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (work 12N^2 + state 8N^2 bytes = 335 MB)"},
+        "mpts_steps_per_s": round(r["value"] * N * N / 1e6, 1),
+        "step_roofline": {"bytes_per_step_survey": 76 * N * N, "bytes_per_step_min": 64 * N * N,
+                          "frac_survey": round(76 * N * N * steps_s / (peak * 1e9), 4),
+                          "frac_min": round(64 * N * N * steps_s / (peak * 1e9), 4)},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": tr, "bytes_per_launch": b, "launch_ms": round(ms, 4)},
+        "kernel_ms": {"k_rows_step": round(r["rows_ms"], 4), "k_cols_step": round(r["cols_ms"], 4)},
+        "gpu_launches": r["kernels"],
+        "clocks": r["clocks"],
+    }
+    if r["e2e"]:
+        line["e2e"] = r["e2e"]
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line), flush=True)
+
+
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    N, K, W = args.n, args.steps, args.warmup
+    exe = os.path.join(REPO, "oracle", "_ref", "mem_cuda")
+    base = {"impl": "reference", "metric": METRIC, "unit": "steps/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"plain DNS N={N} (6144^2 padded grid), Re=1e5, K0=4, CFL=0.1, "
+                                   f"ADAPT_VISC=0, UPDATE={WORKLOAD['UPDATE']}", "N": N}}
+    if os.path.exists(exe):
+        env = dict(os.environ, BENCH_WARMUP_STEPS=str(W))
+        cmd = [exe, str(N), "100000", "4", str(W + K), "0.1", str(WORKLOAD["UPDATE"]), "0"]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+        m = re.search(r"Steady FPS:\s*([0-9.eE+-]+)", p.stdout)
+        if p.returncode != 0 or not m:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              f"reference mem_cuda failed rc={p.returncode}: {p.stderr[-200:]}"}))
+            return
+        v = float(m.group(1))
+        line = dict(base, value=v, ms_per_step=1e3 / v, vs_baseline=None,
+                    mpts_steps_per_s=round(v * N * N / 1e6, 1),
+                    cpu_baseline={"value": v, "unit": "steps/s", "cores": 1, "kind": "reference",
+                                  "sample": f"reference cuFFT build (oracle/_ref/mem_cuda, sm_100a) "
+                                            f"{' '.join(cmd[1:])}, BENCH_WARMUP_STEPS={W}; its own "
+                                            f"'Steady FPS' over {K} steps on cuda:0 ({wall:.1f} s wall)",
+                                  "device": "cuda:0"},
+                    e2e={"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        line["config"]["reference_ic"] = "PAO-k^-3 (the reference CLI's own initialiser)"
+        print(json.dumps(line), flush=True)
+        return
+    cb = cpu_baseline(args)
+    line = dict(base, value=cb["value"], ms_per_step=1e3 / cb["value"], vs_baseline=None,
+                cpu_baseline=cb,
+                e2e={"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        main_reference(a)
+    else:
+        main_ours(a)

@@ -1,0 +1,127 @@
+/*
+ * dns2d.h — C ABI of the B200 (sm_100a) 2D pseudo-spectral vorticity solver.
+ *
+ * Drop-in replacement for the in-process solver API of cudaturbo's mem_cuda
+ * (cuda/cuda_dns.h:108-202).  Plain C types only: every array argument is a host pointer
+ * with an explicit layout, every function returns DNS2D_OK or a DNS2D_ERR_* code (nothing
+ * aborts), and dns2d_last_error() gives the message of the latest failure on a state.
+ *
+ * Grid conventions (the reference's, cuda/cuda_dns.h:27-34, cuda/step3_cuda.cu:57-65):
+ *   N      base resolution (multiple of 8), retained modes |kx| < N/2, -N/2 <= kz < N/2
+ *   L      = 3N/2, the dealiased physical grid (NX_full = NZ_full)
+ *   om2    vorticity spectrum, [iz][ix] complex64 (N rows of N/2), kz = iz < N/2 ? iz : iz-N
+ *   fnm1   previous nonlinear term, same layout
+ *   phys   physical planes [L][L] float32, x fastest: comp 0 = u, 1 = w, 2 = scalar (omega,
+ *          stream function or |u| after the matching call)
+ * A state owns one CUDA stream; calls on one state must come from one host thread.
+ */
+#ifndef DNS2D_H
+#define DNS2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DNS2D_OK = 0,
+    DNS2D_ERR_ARG = 1,      /* bad argument (NULL pointer, wrong size, bad component) */
+    DNS2D_ERR_SIZE = 2,     /* N not supported by the compiled kernels */
+    DNS2D_ERR_CUDA = 3,     /* CUDA runtime error (message in dns2d_last_error) */
+    DNS2D_ERR_NOMEM = 4,    /* device allocation failed */
+    DNS2D_ERR_IO = 5,       /* file could not be opened / read / written */
+    DNS2D_ERR_FORMAT = 6,   /* restart file header or sizes do not match */
+    DNS2D_ERR_STATE = 7,    /* call out of order (e.g. step before an initial condition) */
+    DNS2D_ERR_TIMEOUT = 8   /* host watchdog expired waiting for the device */
+};
+
+typedef struct dns2d_state dns2d_state;
+
+/* Scalars of the run; the float fields follow the reference's float host arithmetic. */
+typedef struct {
+    int32_t N, NX_full, NK_full, it, ifn;
+    float Re, K0, visc, t, dt, cn, cnm1, cflnum, cflm;
+} dns2d_scalars;
+
+/* ---- life cycle: replaces dnsCudaCreate / dnsCudaDestroy (cuda/cuda_dns.h:108-109) ---- */
+int dns2d_create(dns2d_state **out, int N, float Re, float K0, float cflnum, int device);
+void dns2d_destroy(dns2d_state *s);
+const char *dns2d_strerror(int code);
+const char *dns2d_last_error(const dns2d_state *s);
+/* 1 when N is supported by this build, else 0 */
+int dns2d_supported(int N);
+/* device bytes held by a state of size N */
+size_t dns2d_device_bytes(int N);
+
+/* ---- initial conditions: replace dnsCudaInit = PAO + CALCOM (cuda/cuda_dns.h:118-127) ----
+ * All set it = 0, t = 0, dt = 0, cn = 1, cnm1 = 0, and leave the velocity ready, so the next
+ * call is dns2d_next_dt() (the reference's initial STEP2A + NEXTDT init branch). */
+/* PAO-k^-3 field of cuda/pao_km3_cuda.cu:59-498; stats19 (nullable) receives the 19 printed
+ * statistics (Reynolds n., Energy, WiWi, Epsilon, a11, e11, Time scale, Kolmogorov,
+ * Viscosity, dx/Kol., 2Pi/Nlamda, 2Pi/Lux, 2Pi/Luz, 2Pi/Lwx, 2Pi/Lwz, Deps., Ceps2, E1, E3),
+ * pao_seed (nullable) the final generator state ("PAO seed"). */
+int dns2d_init_pao(dns2d_state *s, double *stats19, int *pao_seed);
+/* given vorticity (and optional previous nonlinear term, NULL = 0), [iz][ix] complex64 */
+int dns2d_init_vorticity(dns2d_state *s, const float *om2, const float *fnm1);
+/* seeded random-phase spectrum E(k) ~ (k/K0)^4 exp(-2 (k/K0)^2), total energy 1/2 (no
+ * counterpart in the reference; written for the benchmark configurations) */
+int dns2d_init_k4(dns2d_state *s, uint64_t seed);
+/* the same field on the host without a state: om2 [N][N/2] complex64 */
+int dns2d_k4_spectrum(int N, float K0, uint64_t seed, float *om2);
+
+/* ---- time stepping: replaces dnsCudaStep2B + dnsCudaStep3 + dnsCudaStep2A and the host
+ * bookkeeping of the mem_cuda loop (cuda/mem_cuda.cu:1848-1857).  Advances nsteps steps with
+ * the current dt; per step it += 1, t += dt (float), cnm1 <- cn.  E_hist / Z_hist (nullable,
+ * nsteps entries) receive the FP64 energy 1/2 sum w|om|^2/K^2 and enstrophy 1/2 sum w|om|^2
+ * (w = 1 on kx = 0, else 2) after each step.  Asynchronous unless a history is requested. */
+int dns2d_step(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist);
+/* NEXTDT of cuda/dns_cuda.cu:553-580 on the current velocity; writes CFLM (nullable) */
+int dns2d_next_dt(dns2d_state *s, float *cflm);
+/* the state's CUDA stream (a cudaStream_t), for callers that order their own work after it */
+void *dns2d_stream(dns2d_state *s);
+/* wait for the state's stream; watchdog: DNS2D_ERR_TIMEOUT after timeout_ms (<= 0: none) */
+int dns2d_sync(dns2d_state *s, int timeout_ms);
+
+/* ---- diagnostics ---- */
+/* omega to physical space into phys[2] (dnsCudaOm2Phys, cuda/om2phys_cuda.cu:153-205) */
+int dns2d_om2phys(dns2d_state *s);
+/* stream function psi = om/K^2 into phys[2] (dnsCudaStreamFunc, cuda/om2phys_cuda.cu:258) */
+int dns2d_stream_func(dns2d_state *s);
+/* u, w into phys[0], phys[1] (the reference's UR_full after STEP2A) */
+int dns2d_velocity_phys(dns2d_state *s);
+/* |u| into phys[2] from phys[0..1] (dnsCudaKinetic, cuda/om2phys_cuda.cu:358) */
+int dns2d_kinetic(dns2d_state *s);
+/* std-dev of the 8-bit quantised phys[comp] image (computeDisplaySigma, cuda/mem_cuda.cu:820) */
+int dns2d_display_sigma(dns2d_state *s, int comp, double *sigma);
+/* FP64 energy and enstrophy of the current vorticity */
+int dns2d_energy_enstrophy(dns2d_state *s, double *E, double *Z);
+/* FP64 shell spectrum E(k) = 1/2 sum_{round|k| = k} w |om|^2 / K^2, k = 0..nbins-1 */
+int dns2d_shell_spectrum(dns2d_state *s, double *Ek, int nbins);
+/* palinstrophy ratio of cuda/mem_cuda.cu:872-940 (FP64 on the device) */
+int dns2d_palin(dns2d_state *s, double *pal_over_ens_kmax2);
+/* energy_spectrum.csv bins of cuda/mem_cuda.cu:575-649 from phys[0..1] (nbins = 3N) */
+int dns2d_velocity_spectrum_bins(dns2d_state *s, double *esum, int *count, int nbins);
+
+/* ---- state transfer ---- */
+int dns2d_get_scalars(const dns2d_state *s, dns2d_scalars *out);
+int dns2d_set_scalars(dns2d_state *s, const dns2d_scalars *in);
+int dns2d_get_om2(dns2d_state *s, float *om2);
+int dns2d_get_fnm1(dns2d_state *s, float *fnm1);
+int dns2d_get_phys(dns2d_state *s, int comp, float *plane);
+/* load u, w physical planes (e.g. a restart file's UR_full) as the current velocity */
+int dns2d_set_velocity_phys(dns2d_state *s, const float *u, const float *w);
+/* restart.bin v2 writer / v1+v2 reader (cuda/mem_cuda.cu:1019-1394 byte layout) */
+int dns2d_save_restart(dns2d_state *s, const char *path);
+int dns2d_load_restart(dns2d_state *s, const char *path);
+
+/* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
+int dns2d_phase_timing(dns2d_state *s, int enable);
+/* ms[0..3], counts[0..3]: row pass, column pass, NEXTDT/CFLM, OM2PHYS+sigma */
+int dns2d_phase_report(dns2d_state *s, double *ms, long long *counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DNS2D_H */

@@ -1,0 +1,311 @@
+"""optimizec_b200 — B200 (sm_100a) replacement for cudaturbo's 2D pseudo-spectral vorticity step.
+
+The product is the C ABI library ``libdns2d.so`` (declared in ``include/dns2d.h``) and the
+drop-in ``mem_cuda`` CLI.  This module is a thin ctypes front end over that library, with one
+method per entry point of the reference's in-process solver API (cuda/cuda_dns.h:108-202):
+
+    reference (cuda_dns.h)            here
+    dnsCudaCreate / dnsCudaDestroy    Solver(N, Re, K0, cfl) / Solver.close()
+    dnsCudaInit (PAO + CALCOM)        Solver.init_pao()
+    dnsCudaStep2B/Step3/Step2A        Solver.step(n)
+    next_dt_gpu                       Solver.next_dt()
+    dnsCudaOm2Phys                    Solver.om2phys()
+    dnsCudaStreamFunc / Kinetic       Solver.stream_func() / Solver.kinetic()
+
+Errors raise ``Dns2dError`` with the library's message; there is no CPU fallback: if the
+shared library or a CUDA device is missing the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdns2d.so")
+REPO = os.path.dirname(_HERE)
+
+SYMBOLS = [
+    "dns2d_create", "dns2d_destroy", "dns2d_strerror", "dns2d_last_error", "dns2d_supported",
+    "dns2d_device_bytes", "dns2d_init_pao", "dns2d_init_vorticity", "dns2d_init_k4",
+    "dns2d_k4_spectrum", "dns2d_step", "dns2d_next_dt", "dns2d_stream", "dns2d_sync", "dns2d_om2phys",
+    "dns2d_stream_func", "dns2d_velocity_phys", "dns2d_kinetic", "dns2d_display_sigma",
+    "dns2d_energy_enstrophy", "dns2d_shell_spectrum", "dns2d_palin",
+    "dns2d_velocity_spectrum_bins", "dns2d_get_scalars", "dns2d_set_scalars", "dns2d_get_om2",
+    "dns2d_get_fnm1", "dns2d_get_phys", "dns2d_set_velocity_phys", "dns2d_save_restart",
+    "dns2d_load_restart", "dns2d_phase_timing", "dns2d_phase_report",
+]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]
+
+
+class Dns2dError(RuntimeError):
+    pass
+
+
+class Scalars(C.Structure):
+    _fields_ = [("N", C.c_int32), ("NX_full", C.c_int32), ("NK_full", C.c_int32),
+                ("it", C.c_int32), ("ifn", C.c_int32), ("Re", C.c_float), ("K0", C.c_float),
+                ("visc", C.c_float), ("t", C.c_float), ("dt", C.c_float), ("cn", C.c_float),
+                ("cnm1", C.c_float), ("cflnum", C.c_float), ("cflm", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libdns2d.so (sm_100a) and the mem_cuda CLI in-tree."""
+    src = os.path.join(_HERE, "csrc", "dns2d_api.cu")
+    cmd = [NVCC, *ARCH, *CUFLAGS, "-Xcompiler", "-fPIC", "-shared", "-o", LIB_PATH, src]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    cli_src = os.path.join(_HERE, "cli", "mem_cuda.cpp")
+    if os.path.exists(cli_src):
+        cli = os.path.join(_HERE, "mem_cuda")
+        cmd = [NVCC, *ARCH, "-O2", "-std=c++17", "-o", cli, cli_src, "-L" + _HERE, "-ldns2d",
+               "-Xlinker", "-rpath,$ORIGIN", "-I" + os.path.join(REPO, "include")]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    """Load libdns2d.so (building it first when absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        build()
+    L = C.CDLL(LIB_PATH)
+    vp, fp, dp, ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
+    sig = {
+        "dns2d_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_float, C.c_float, C.c_float, C.c_int]),
+        "dns2d_destroy": (None, [vp]),
+        "dns2d_strerror": (C.c_char_p, [C.c_int]),
+        "dns2d_last_error": (C.c_char_p, [vp]),
+        "dns2d_supported": (C.c_int, [C.c_int]),
+        "dns2d_device_bytes": (C.c_size_t, [C.c_int]),
+        "dns2d_init_pao": (C.c_int, [vp, dp, ip]),
+        "dns2d_init_vorticity": (C.c_int, [vp, fp, fp]),
+        "dns2d_init_k4": (C.c_int, [vp, C.c_uint64]),
+        "dns2d_k4_spectrum": (C.c_int, [C.c_int, C.c_float, C.c_uint64, fp]),
+        "dns2d_step": (C.c_int, [vp, C.c_int, dp, dp]),
+        "dns2d_next_dt": (C.c_int, [vp, fp]),
+        "dns2d_stream": (vp, [vp]),
+        "dns2d_sync": (C.c_int, [vp, C.c_int]),
+        "dns2d_om2phys": (C.c_int, [vp]),
+        "dns2d_stream_func": (C.c_int, [vp]),
+        "dns2d_velocity_phys": (C.c_int, [vp]),
+        "dns2d_kinetic": (C.c_int, [vp]),
+        "dns2d_display_sigma": (C.c_int, [vp, C.c_int, dp]),
+        "dns2d_energy_enstrophy": (C.c_int, [vp, dp, dp]),
+        "dns2d_shell_spectrum": (C.c_int, [vp, dp, C.c_int]),
+        "dns2d_palin": (C.c_int, [vp, dp]),
+        "dns2d_velocity_spectrum_bins": (C.c_int, [vp, dp, ip, C.c_int]),
+        "dns2d_get_scalars": (C.c_int, [vp, C.POINTER(Scalars)]),
+        "dns2d_set_scalars": (C.c_int, [vp, C.POINTER(Scalars)]),
+        "dns2d_get_om2": (C.c_int, [vp, fp]),
+        "dns2d_get_fnm1": (C.c_int, [vp, fp]),
+        "dns2d_get_phys": (C.c_int, [vp, C.c_int, fp]),
+        "dns2d_set_velocity_phys": (C.c_int, [vp, fp, fp]),
+        "dns2d_save_restart": (C.c_int, [vp, C.c_char_p]),
+        "dns2d_load_restart": (C.c_int, [vp, C.c_char_p]),
+        "dns2d_phase_timing": (C.c_int, [vp, C.c_int]),
+        "dns2d_phase_report": (C.c_int, [vp, dp, C.POINTER(C.c_longlong)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def supported(N: int) -> bool:
+    return bool(lib().dns2d_supported(N))
+
+
+def k4_spectrum(N: int, K0: float, seed: int) -> np.ndarray:
+    out = np.zeros((N, N // 2), dtype=np.complex64)
+    rc = lib().dns2d_k4_spectrum(N, K0, seed, _fp(out.view(np.float32)))
+    if rc:
+        raise Dns2dError(lib().dns2d_strerror(rc).decode())
+    return out
+
+
+class Solver:
+    """One simulation on one GPU (owns a dns2d_state)."""
+
+    def __init__(self, N: int, Re: float, K0: float, cfl: float, device: int = 0):
+        self.N, self.H, self.L = N, N // 2, 3 * N // 2
+        self._L = lib()
+        self._s = C.c_void_p()
+        rc = self._L.dns2d_create(C.byref(self._s), N, Re, K0, cfl, device)
+        if rc:
+            raise Dns2dError(f"dns2d_create(N={N}): {self._L.dns2d_strerror(rc).decode()}")
+
+    def _chk(self, rc):
+        if rc:
+            msg = self._L.dns2d_last_error(self._s).decode() if self._s else ""
+            raise Dns2dError(f"{self._L.dns2d_strerror(rc).decode()}: {msg}")
+
+    def close(self):
+        if self._s:
+            self._L.dns2d_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- initial conditions ----
+    def init_pao(self):
+        stats = np.zeros(19)
+        seed = C.c_int(0)
+        self._chk(self._L.dns2d_init_pao(self._s, _dp(stats), C.byref(seed)))
+        return stats, seed.value
+
+    def init_vorticity(self, om2: np.ndarray, fnm1: np.ndarray | None = None):
+        om2 = np.ascontiguousarray(om2, dtype=np.complex64)
+        f = None if fnm1 is None else np.ascontiguousarray(fnm1, dtype=np.complex64)
+        self._chk(self._L.dns2d_init_vorticity(self._s, _fp(om2.view(np.float32)),
+                                               None if f is None else _fp(f.view(np.float32))))
+
+    def init_k4(self, seed: int):
+        self._chk(self._L.dns2d_init_k4(self._s, seed))
+
+    # ---- stepping ----
+    def step(self, n: int, history: bool = False):
+        if history:
+            E = np.zeros(n)
+            Z = np.zeros(n)
+            self._chk(self._L.dns2d_step(self._s, n, _dp(E), _dp(Z)))
+            return E, Z
+        self._chk(self._L.dns2d_step(self._s, n, None, None))
+        return None
+
+    def next_dt(self) -> float:
+        c = C.c_float(0)
+        self._chk(self._L.dns2d_next_dt(self._s, C.byref(c)))
+        return c.value
+
+    def stream(self) -> int:
+        """the state's cudaStream_t as an integer handle"""
+        return self._L.dns2d_stream(self._s) or 0
+
+    def sync(self, timeout_ms: int = 0):
+        self._chk(self._L.dns2d_sync(self._s, timeout_ms))
+
+    # ---- diagnostics ----
+    def om2phys(self):
+        self._chk(self._L.dns2d_om2phys(self._s))
+
+    def stream_func(self):
+        self._chk(self._L.dns2d_stream_func(self._s))
+
+    def velocity_phys(self):
+        self._chk(self._L.dns2d_velocity_phys(self._s))
+
+    def kinetic(self):
+        self._chk(self._L.dns2d_kinetic(self._s))
+
+    def display_sigma(self, comp: int = 2) -> float:
+        v = C.c_double(0)
+        self._chk(self._L.dns2d_display_sigma(self._s, comp, C.byref(v)))
+        return v.value
+
+    def energy_enstrophy(self):
+        E, Z = C.c_double(0), C.c_double(0)
+        self._chk(self._L.dns2d_energy_enstrophy(self._s, C.byref(E), C.byref(Z)))
+        return E.value, Z.value
+
+    def shell_spectrum(self, nb: int | None = None) -> np.ndarray:
+        nb = nb or (self.N // 2 + self.N // 4 + 2)
+        out = np.zeros(nb)
+        self._chk(self._L.dns2d_shell_spectrum(self._s, _dp(out), nb))
+        return out
+
+    def palin(self) -> float:
+        v = C.c_double(0)
+        self._chk(self._L.dns2d_palin(self._s, C.byref(v)))
+        return v.value
+
+    def velocity_spectrum_bins(self, nbins: int | None = None):
+        nbins = nbins or max(32, 2 * self.L)
+        e = np.zeros(nbins)
+        c = np.zeros(nbins, dtype=np.int32)
+        self._chk(self._L.dns2d_velocity_spectrum_bins(self._s, _dp(e), c.ctypes.data_as(C.POINTER(C.c_int)), nbins))
+        return e, c
+
+    # ---- state ----
+    def scalars(self) -> dict:
+        s = Scalars()
+        self._chk(self._L.dns2d_get_scalars(self._s, C.byref(s)))
+        return s.as_dict()
+
+    def set_scalars(self, **kw):
+        s = Scalars()
+        self._chk(self._L.dns2d_get_scalars(self._s, C.byref(s)))
+        for k, v in kw.items():
+            setattr(s, k, v)
+        self._chk(self._L.dns2d_set_scalars(self._s, C.byref(s)))
+
+    def om2(self) -> np.ndarray:
+        out = np.zeros((self.N, self.H), dtype=np.complex64)
+        self._chk(self._L.dns2d_get_om2(self._s, _fp(out.view(np.float32))))
+        return out
+
+    def fnm1(self) -> np.ndarray:
+        out = np.zeros((self.N, self.H), dtype=np.complex64)
+        self._chk(self._L.dns2d_get_fnm1(self._s, _fp(out.view(np.float32))))
+        return out
+
+    def phys(self, comp: int) -> np.ndarray:
+        out = np.zeros((self.L, self.L), dtype=np.float32)
+        self._chk(self._L.dns2d_get_phys(self._s, comp, _fp(out)))
+        return out
+
+    def set_velocity_phys(self, u: np.ndarray, w: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float32)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._chk(self._L.dns2d_set_velocity_phys(self._s, _fp(u), _fp(w)))
+
+    def save_restart(self, path: str):
+        self._chk(self._L.dns2d_save_restart(self._s, path.encode()))
+
+    def load_restart(self, path: str):
+        self._chk(self._L.dns2d_load_restart(self._s, path.encode()))
+
+    def phase_timing(self, on: bool):
+        self._chk(self._L.dns2d_phase_timing(self._s, int(on)))
+
+    def phase_report(self):
+        ms = np.zeros(4)
+        n = np.zeros(4, dtype=np.int64)
+        self._chk(self._L.dns2d_phase_report(self._s, _dp(ms), n.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return ms, n

@@ -1,0 +1,1390 @@
+// dns2d_api.cu — host side of the B200 2D vorticity solver: the C ABI of include/dns2d.h.
+//
+// The state owns its device buffers, one non-blocking CUDA stream and a cache of captured CUDA
+// graphs (one per segment length).  The scalar bookkeeping (it, t, dt, cn, cnm1, cflm) is kept
+// on the host in float and updated with the same expressions, in the same order, as the
+// reference's host code (cuda/mem_cuda.cu:1848-1862, cuda/dns_cuda.cu:553-580,
+// cuda/step3_cuda.cu:172), so printed T/DT/CN values follow the reference.  The device sees
+// dt/cn/cnm1 through a small parameter block written by a one-thread kernel at the start of
+// every dns2d_step call, which lets one captured graph serve every segment.
+#include "dns2d_kernels.cuh"
+#include "../../include/dns2d.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace dns2d;
+
+// ============================================================================================
+// kernel sets, one per compiled N
+// ============================================================================================
+namespace {
+
+struct KernelSet {
+    int N;
+    int rows_blocks;
+    cudaError_t (*setup)();
+    void (*rows_step)(const Pointers &, cudaStream_t);
+    void (*cols_step)(const Pointers &, int, int, cudaStream_t);
+    void (*cols_init)(const Pointers &, const float2 *, int, cudaStream_t);
+    void (*rows_velocity)(const Pointers &, float *, float *, float, cudaStream_t);
+    void (*rows_from_phys)(const Pointers &, const float *, cudaStream_t);
+    void (*cols_scalar)(const Pointers &, float2 *, int, cudaStream_t);
+    void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
+};
+
+template <int N>
+struct Launch {
+    using C = Cfg<N>;
+    static constexpr size_t smB = (size_t)C::ROWS * C::LP * sizeof(float2);
+    static constexpr size_t smA = (size_t)2 * C::LP * sizeof(float2);
+    static constexpr size_t smA1 = (size_t)C::LP * sizeof(float2);
+    static constexpr int GB = C::L / C::ROWS;
+
+    static cudaError_t setup()
+    {
+        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_rows_step<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_init<N>, a, (int)smA)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_velocity<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_from_phys<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
+        return cudaSuccess;
+    }
+    static void rows_step(const Pointers &p, cudaStream_t s) { k_rows_step<N><<<GB, C::NTB, smB, s>>>(p); }
+    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s)
+    {
+        k_cols_step<N><<<C::H, C::NTA, smA, s>>>(p, first, slot);
+    }
+    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s)
+    {
+        k_cols_init<N><<<C::H, C::NTA, smA, s>>>(p, uw, mode);
+    }
+    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s)
+    {
+        k_rows_velocity<N><<<GB, C::NTB, smB, s>>>(p, phys, cflm, dx);
+    }
+    static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
+    {
+        k_rows_from_phys<N><<<GB, C::NTB, smB, s>>>(p, phys);
+    }
+    static void cols_scalar(const Pointers &p, float2 *scratch, int kind, cudaStream_t s)
+    {
+        k_cols_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, kind);
+    }
+    static void rows_scalar(const Pointers &p, const float2 *scratch, float *out, float2 *mm, cudaStream_t s)
+    {
+        k_rows_scalar<N><<<GB, C::NTB, smB, s>>>(p, scratch, out, mm);
+    }
+    static KernelSet make()
+    {
+        return KernelSet{N, GB, setup, rows_step, cols_step, cols_init, rows_velocity, rows_from_phys,
+                         cols_scalar, rows_scalar};
+    }
+};
+
+const KernelSet *kernel_set(int N)
+{
+    static const KernelSet sets[] = {
+        Launch<16>::make(),   Launch<32>::make(),   Launch<64>::make(),
+        Launch<128>::make(),  Launch<256>::make(),  Launch<512>::make(),
+        Launch<1024>::make(), Launch<2048>::make(), Launch<4096>::make(),
+    };
+    for (const KernelSet &k : sets)
+        if (k.N == N) return &k;
+    return nullptr;
+}
+
+// ============================================================================================
+// small non-templated kernels
+// ============================================================================================
+__global__ void k_set_params(StepParams *prm, float dt, float cnm1_first, float cn, float visc)
+{
+    prm->dt = dt;
+    prm->cnm1_first = cnm1_first;
+    prm->cn = cn;
+    prm->visc = visc;
+}
+
+// |u| into phys[2] (cuda/om2phys_cuda.cu:331-355)
+__global__ void k_kinetic(float *phys, size_t plane)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
+        const float u = phys[i], w = phys[plane + i];
+        phys[2 * plane + i] = sqrtf(u * u + w * w);
+    }
+}
+
+__global__ void k_minmax(const float *f, size_t n, float2 *out)
+{
+    __shared__ float smn[256], smx[256];
+    float mn = 3.402823466e38f, mx = -3.402823466e38f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = f[i];
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+    smn[threadIdx.x] = mn;
+    smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            smn[threadIdx.x] = fminf(smn[threadIdx.x], smn[threadIdx.x + o]);
+            smx[threadIdx.x] = fmaxf(smx[threadIdx.x], smx[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = make_float2(smn[0], smx[0]);
+}
+
+// 8-bit display quantisation sums (cuda/mem_cuda.cu:691-740): same IEEE operation sequence
+__global__ void k_sigma_pixels(const float *f, size_t n, float minv, float rng, int is_constant,
+                               unsigned long long *sums)
+{
+    __shared__ unsigned long long s1[256], s2[256];
+    unsigned long long a = 0, b = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int pix = 128;
+        if (!is_constant) {
+            const float norm = __fdiv_rn(__fsub_rn(f[i], minv), rng);
+            float pf = __fadd_rn(1.0f, __fmul_rn(norm, 254.0f));
+            if (pf < 1.0f) pf = 1.0f;
+            if (pf > 255.0f) pf = 255.0f;
+            pix = (int)pf;
+        }
+        a += (unsigned long long)pix;
+        b += (unsigned long long)(pix * pix);
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sums[2 * blockIdx.x] = s1[0];
+        sums[2 * blockIdx.x + 1] = s2[0];
+    }
+}
+
+// FP64 reductions over the [kx][kz] vorticity: out[block] = {E, Z, pal, total_full, k00, kmax2}
+__global__ void k_om2_reduce(const float2 *om2, int N, double *out)
+{
+    const int H = N / 2;
+    __shared__ double sh[6][256];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const size_t n = (size_t)N * H;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(i / N), iz = (int)(i % N);
+        const int kz = (iz < H) ? iz : iz - N;
+        const float2 o = om2[i];
+        const double p = (double)o.x * o.x + (double)o.y * o.y;
+        const double k2 = (double)kx * kx + (double)kz * kz;
+        const double w = (kx == 0) ? 1.0 : 2.0;
+        acc[1] += 0.5 * w * p;
+        if (k2 > 0) acc[0] += 0.5 * w * p / k2;
+        // palinstrophy weights of cuda/mem_cuda.cu:912-916 (1 on x = 0 and x = N/2-1)
+        const double wp = (kx == 0 || kx == H - 1) ? 1.0 : 2.0;
+        acc[2] += wp * k2 * p;
+        acc[3] += wp * p;
+        if (kx == 0 && iz == 0) acc[4] += p;
+        acc[5] = fmax(acc[5], k2);
+    }
+    for (int j = 0; j < 6; ++j) sh[j][threadIdx.x] = acc[j];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            for (int j = 0; j < 5; ++j) sh[j][threadIdx.x] += sh[j][threadIdx.x + o];
+            sh[5][threadIdx.x] = fmax(sh[5][threadIdx.x], sh[5][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int j = 0; j < 6; ++j) out[6 * blockIdx.x + j] = sh[j][0];
+}
+
+__global__ void k_shell(const float2 *om2, int N, double *Ek, int nb)
+{
+    const int H = N / 2;
+    const size_t n = (size_t)N * H;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(i / N), iz = (int)(i % N);
+        const int kz = (iz < H) ? iz : iz - N;
+        const double k2 = (double)kx * kx + (double)kz * kz;
+        if (k2 == 0.0) continue;
+        const int sh = (int)(sqrt(k2) + 0.5);
+        if (sh >= nb) continue;
+        const float2 o = om2[i];
+        const double w = (kx == 0) ? 1.0 : 2.0;
+        atomicAdd(&Ek[sh], 0.5 * w * ((double)o.x * o.x + (double)o.y * o.y) / k2);
+    }
+}
+
+// energy_spectrum.csv bins (cuda/mem_cuda.cu:593-629) over the full L x (L/2+1) grid.  The
+// velocity is band limited, so F[u](kz,kx) = L^2 u_hat for retained modes and 0 elsewhere;
+// every grid mode is still counted, as in the reference.
+__global__ void k_vel_bins(const float2 *om2, int N, double *esum, int *cnt, int nbins)
+{
+    const int H = N / 2, L = 3 * N / 2, Nk = L / 2 + 1;
+    const double r_max = sqrt(2.0), k_nyq = 0.5 * (double)L;
+    const double L2 = (double)L * (double)L;
+    const size_t n = (size_t)L * Nk;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i / Nk), kx = (int)(i % Nk);
+        const int kz = (z <= L / 2) ? z : z - L;
+        if (kx == 0 && kz == 0) continue;
+        const double r = sqrt((double)kx * kx + (double)kz * kz) / k_nyq;
+        int bin = (int)floor((r / r_max) * nbins);
+        if (bin < 0) bin = 0;
+        if (bin >= nbins) bin = nbins - 1;
+        const bool dbl = (kx > 0 && 2 * kx < L);
+        atomicAdd(&cnt[bin], dbl ? 2 : 1);
+        if (kx < H && kz >= -H && kz < H) {
+            const int iz = (kz >= 0) ? kz : kz + N;
+            const float2 o = om2[(size_t)kx * N + iz];
+            const double K2 = (double)kx * kx + (double)kz * kz;
+            const double ox = o.x, oy = o.y;
+            double uu, ww;
+            if (kx >= 1) {
+                uu = (double)kz * kz * (ox * ox + oy * oy) / (K2 * K2);
+                ww = (double)kx * kx * (ox * ox + oy * oy) / (K2 * K2);
+            } else {
+                uu = (kz != 0) ? (ox * ox + oy * oy) / ((double)kz * kz) : 0.0;
+                ww = 0.0;
+            }
+            double p = (uu + ww) * L2 * L2;
+            if (dbl) p *= 2.0;
+            if (p != 0.0) atomicAdd(&esum[bin], p);
+        }
+    }
+}
+
+// [iz][ix] <-> [ix][iz] transposes of the compact spectra
+__global__ void k_transpose_c64(const float2 *in, float2 *out, int rows, int cols)
+{
+    __shared__ float2 t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = by + j, c = bx + threadIdx.x;
+        if (r < rows && c < cols) t[j][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int c = bx + j, r = by + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = t[threadIdx.x][j];
+    }
+}
+
+}  // namespace
+
+// ============================================================================================
+// state
+// ============================================================================================
+struct dns2d_state {
+    int N = 0, H = 0, L = 0, Nk = 0, device = 0;
+    float Re = 0, K0 = 0, visc = 0, t = 0, dt = 0, cn = 1, cnm1 = 0, cflnum = 0, cflm = 0;
+    int it = 0, ifn = 1;
+    bool initialised = false;
+    const KernelSet *ks = nullptr;
+    cudaStream_t stream = nullptr;
+    // device buffers
+    float2 *om2 = nullptr, *fnm1 = nullptr, *work = nullptr, *tw = nullptr, *scratch = nullptr;
+    float *phys = nullptr;
+    StepParams *prm = nullptr;
+    double2 *part = nullptr, *hist = nullptr;
+    unsigned int *counter = nullptr;
+    float *cflm_dev = nullptr;
+    float2 *minmax = nullptr;
+    unsigned long long *sums = nullptr;
+    double *red = nullptr;
+    int hist_cap = 0;
+    // pinned host
+    double2 *hist_host = nullptr;
+    // graphs keyed by (first, K)
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    // phase timing
+    bool timing = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double phase_ms[4] = {0, 0, 0, 0};
+    long long phase_n[4] = {0, 0, 0, 0};
+    std::string err;
+
+    Pointers ptrs() const
+    {
+        Pointers p;
+        p.om2 = om2;
+        p.fnm1 = fnm1;
+        p.work = work;
+        p.tw = tw;
+        p.prm = prm;
+        p.part = part;
+        p.counter = counter;
+        p.hist = hist;
+        return p;
+    }
+};
+
+namespace {
+
+constexpr int kHistCap = 4096;
+constexpr int kSigmaBlocks = 1024;
+constexpr int kRedBlocks = 512;
+constexpr int kChunk = 128;  // steps per captured graph
+
+int fail(dns2d_state *s, int code, const char *fmt, ...)
+{
+    if (s) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        s->err = buf;
+    }
+    return code;
+}
+
+int cuda_check(dns2d_state *s, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return DNS2D_OK;
+    return fail(s, DNS2D_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define DNS2D_CUDA(call, what)                                      \
+    do {                                                            \
+        int rc_ = cuda_check(s, (call), what);                      \
+        if (rc_ != DNS2D_OK) return rc_;                            \
+    } while (0)
+
+#define DNS2D_LAUNCHED(what) DNS2D_CUDA(cudaGetLastError(), what)
+
+void free_graphs(dns2d_state *s)
+{
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+}
+
+// twiddle table W_L^j = exp(-2 pi i j/L) built in FP64 and rounded once
+std::vector<float2> twiddles(int L)
+{
+    std::vector<float2> t((size_t)L);
+    for (int j = 0; j < L; ++j) {
+        // exact symmetric reduction of the angle to the first octant-free form
+        const double a = 2.0 * M_PI * (double)j / (double)L;
+        t[(size_t)j] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    return t;
+}
+
+void phase_begin(dns2d_state *s)
+{
+    if (s->timing) cudaEventRecord(s->ev0, s->stream);
+}
+
+void phase_end(dns2d_state *s, int id)
+{
+    if (!s->timing) return;
+    cudaEventRecord(s->ev1, s->stream);
+    cudaEventSynchronize(s->ev1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->phase_ms[id] += ms;
+    s->phase_n[id] += 1;
+}
+
+}  // namespace
+
+// ============================================================================================
+// life cycle
+// ============================================================================================
+extern "C" const char *dns2d_strerror(int code)
+{
+    switch (code) {
+    case DNS2D_OK: return "ok";
+    case DNS2D_ERR_ARG: return "invalid argument";
+    case DNS2D_ERR_SIZE: return "unsupported grid size";
+    case DNS2D_ERR_CUDA: return "CUDA error";
+    case DNS2D_ERR_NOMEM: return "device allocation failed";
+    case DNS2D_ERR_IO: return "file I/O error";
+    case DNS2D_ERR_FORMAT: return "restart format mismatch";
+    case DNS2D_ERR_STATE: return "call out of order";
+    case DNS2D_ERR_TIMEOUT: return "device watchdog timeout";
+    default: return "unknown error";
+    }
+}
+
+extern "C" const char *dns2d_last_error(const dns2d_state *s) { return s ? s->err.c_str() : "null state"; }
+
+extern "C" int dns2d_supported(int N) { return kernel_set(N) != nullptr ? 1 : 0; }
+
+extern "C" size_t dns2d_device_bytes(int N)
+{
+    const size_t H = N / 2, L = 3 * (size_t)N / 2;
+    return 2 * (size_t)N * H * 8      // om2, fnm1
+           + 2 * L * H * 8            // work
+           + L * H * 8                // scratch
+           + 3 * L * L * 4            // phys
+           + L * 8 + H * 16 + kHistCap * 16;
+}
+
+extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float cflnum, int device)
+{
+    if (!out) return DNS2D_ERR_ARG;
+    *out = nullptr;
+    const KernelSet *ks = kernel_set(N);
+    if (!ks) return DNS2D_ERR_SIZE;
+    dns2d_state *s = new dns2d_state();
+    s->N = N;
+    s->H = N / 2;
+    s->L = 3 * N / 2;
+    s->Nk = 3 * N / 4 + 1;
+    s->Re = Re;
+    s->K0 = K0;
+    s->visc = 0.0f;
+    s->cflnum = cflnum;
+    s->device = device;
+    s->ks = ks;
+    auto bail = [&](int rc) {
+        dns2d_destroy(s);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (ks->setup() != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    const size_t H = s->H, L = s->L;
+    const size_t nom = (size_t)N * H;
+    auto dalloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+    if (!dalloc((void **)&s->om2, nom * 8) || !dalloc((void **)&s->fnm1, nom * 8) ||
+        !dalloc((void **)&s->work, 2 * L * H * 8) || !dalloc((void **)&s->scratch, L * H * 8) ||
+        !dalloc((void **)&s->phys, 3 * L * L * 4) || !dalloc((void **)&s->tw, L * 8) ||
+        !dalloc((void **)&s->prm, sizeof(StepParams)) || !dalloc((void **)&s->part, H * 16) ||
+        !dalloc((void **)&s->hist, (size_t)kHistCap * 16) || !dalloc((void **)&s->counter, 4) ||
+        !dalloc((void **)&s->cflm_dev, 4) || !dalloc((void **)&s->minmax, (size_t)std::max(kSigmaBlocks, ks->rows_blocks) * 8) ||
+        !dalloc((void **)&s->sums, (size_t)kSigmaBlocks * 16) || !dalloc((void **)&s->red, (size_t)kRedBlocks * 6 * 8)) {
+        cudaGetLastError();
+        return bail(DNS2D_ERR_NOMEM);
+    }
+    s->hist_cap = kHistCap;
+    if (cudaMallocHost((void **)&s->hist_host, (size_t)kHistCap * 16) != cudaSuccess) return bail(DNS2D_ERR_NOMEM);
+    std::vector<float2> tw = twiddles(s->L);
+    if (cudaMemcpy(s->tw, tw.data(), L * 8, cudaMemcpyHostToDevice) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaMemset(s->counter, 0, 4) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaMemset(s->om2, 0, nom * 8) != cudaSuccess || cudaMemset(s->fnm1, 0, nom * 8) != cudaSuccess ||
+        cudaMemset(s->work, 0, 2 * L * H * 8) != cudaSuccess || cudaMemset(s->phys, 0, 3 * L * L * 4) != cudaSuccess)
+        return bail(DNS2D_ERR_CUDA);
+    if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    *out = s;
+    return DNS2D_OK;
+}
+
+extern "C" void dns2d_destroy(dns2d_state *s)
+{
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_graphs(s);
+    cudaFree(s->om2);
+    cudaFree(s->fnm1);
+    cudaFree(s->work);
+    cudaFree(s->scratch);
+    cudaFree(s->phys);
+    cudaFree(s->tw);
+    cudaFree(s->prm);
+    cudaFree(s->part);
+    cudaFree(s->hist);
+    cudaFree(s->counter);
+    cudaFree(s->cflm_dev);
+    cudaFree(s->minmax);
+    cudaFree(s->sums);
+    cudaFree(s->red);
+    if (s->hist_host) cudaFreeHost(s->hist_host);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+// ============================================================================================
+// initial conditions
+// ============================================================================================
+namespace {
+
+void reset_scalars(dns2d_state *s)
+{
+    s->it = 0;
+    s->t = 0.0f;
+    s->dt = 0.0f;
+    s->cn = 1.0f;
+    s->cnm1 = 0.0f;
+    s->ifn = 1;
+}
+
+// upload [iz][ix] c64 host arrays into the [kx][kz] device layout
+int upload_compact(dns2d_state *s, const float *host, float2 *dst)
+{
+    const size_t n = (size_t)s->N * s->H;
+    DNS2D_CUDA(cudaMemcpyAsync(s->scratch, host, n * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    dim3 b(32, 8), g((s->H + 31) / 32, (s->N + 31) / 32);
+    k_transpose_c64<<<g, b, 0, s->stream>>>(s->scratch, dst, s->N, s->H);
+    DNS2D_LAUNCHED("transpose");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "upload sync");
+    return DNS2D_OK;
+}
+
+int download_compact(dns2d_state *s, const float2 *src, float *host)
+{
+    const size_t n = (size_t)s->N * s->H;
+    dim3 b(32, 8), g((s->N + 31) / 32, (s->H + 31) / 32);
+    k_transpose_c64<<<g, b, 0, s->stream>>>(src, s->scratch, s->H, s->N);
+    DNS2D_LAUNCHED("transpose");
+    DNS2D_CUDA(cudaMemcpyAsync(host, s->scratch, n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "download sync");
+    return DNS2D_OK;
+}
+
+// PAO-k^-3 host initial condition with the reference's float/double arithmetic
+// (cuda/pao_km3_cuda.cu:59-424).  uw: [z][x][2] complex float.
+void pao_host(int N, float K0, float Re, std::vector<std::complex<float>> &uw, double *stats, int *seed_out)
+{
+    const int NE = N, ND2 = N / 2, NED2 = NE / 2;
+    const float PI = 3.14159265358979f;
+    const float DXZ = 2.0f * PI / float(N);
+    const float NORM = PI * K0 * K0;
+    const float AMP2_FLOOR = 1.0e-40f;
+    std::vector<float> alfa(ND2), gamma(NE);
+    const float E1 = 1.0f, E3 = 1.0f / E1;
+    for (int x = 0; x < NED2; ++x) alfa[x] = float(x) * (1.0f / E1);
+    gamma[0] = 0.0f;
+    for (int z = 1; z <= NED2; ++z) {
+        gamma[z] = float(z) * (1.0f / E3);
+        gamma[NE - z] = -gamma[z];
+    }
+    uw.assign((size_t)ND2 * NE * 2, std::complex<float>(0.0f, 0.0f));
+    auto at = [&](int x, int z, int c) -> std::complex<float> & { return uw[(size_t)c + 2 * ((size_t)x + (size_t)ND2 * z)]; };
+
+    // Fortran-style LCG and the 97-entry shuffle table
+    int seed = 1;
+    const int seed_init = 1;
+    auto frand = [&]() {
+        seed = (seed * 420029 + 2017) % 5011;
+        return float(seed) / float(5011);
+    };
+    float ranvec[97];
+    for (int i = 0; i < 97; ++i) frand();
+    for (int i = 0; i < 97; ++i) ranvec[i] = frand();
+    for (int z = 0; z < NE; ++z) {
+        for (int x = 0; x < NED2; ++x) {
+            const float r = frand();
+            int idx = int(r * 97.0f);
+            idx = std::min(96, std::max(0, idx));
+            const float pick = ranvec[idx];
+            ranvec[idx] = r;
+            const float th = 2.0f * PI * pick;
+            const std::complex<float> arg(std::cos(th), std::sin(th));
+            const float ax = alfa[x], gz = gamma[z];
+            const float K = std::sqrt(ax * ax + gz * gz);
+            if (ax == 0.0f) {
+                at(x, z, 1) = std::complex<float>(0.0f, 0.0f);
+                float a2 = std::exp(-(K / K0) * (K / K0)) / NORM;
+                if (a2 < AMP2_FLOOR) a2 = AMP2_FLOOR;
+                at(x, z, 0) = std::sqrt(a2) * arg;
+            } else {
+                const float denom = 1.0f + (gz * gz) / (ax * ax);
+                float a2 = std::exp(-(K / K0) * (K / K0)) / (denom * NORM);
+                if (a2 < AMP2_FLOOR) a2 = AMP2_FLOOR;
+                const std::complex<float> w = std::sqrt(a2) * arg;
+                at(x, z, 1) = w;
+                at(x, z, 0) = -(gz / ax) * w;
+            }
+        }
+    }
+    at(0, 0, 0) = at(0, 0, 1) = std::complex<float>(0.0f, 0.0f);
+    for (int z = 1; z < NED2; ++z) {
+        at(0, NE - z, 0) = std::conj(at(0, z, 0));
+        at(0, NE - z, 1) = std::conj(at(0, z, 1));
+    }
+    for (int x = 0; x < ND2; ++x) at(x, NED2, 0) = at(x, NED2, 1) = std::complex<float>(0.0f, 0.0f);
+
+    // shell re-weighting toward E(k) ~ k^-3 with hashed jitter and phases
+    auto hash01 = [](int x, int z, int sd, int salt) {
+        const double a = (double(x) + 1.0) * 12.9898 + (double(z) + 1.0) * 78.233 +
+                         (double(sd) + 1.0) * 0.010001 + (double(salt) + 1.0) * 37.719;
+        const double v = std::sin(a) * 43758.5453123;
+        return v - std::floor(v);
+    };
+    const double knyq = double(ND2);
+    const int kmax = ND2;
+    std::vector<double> shell_e(kmax + 1, 0.0), shell_w(kmax + 1, 0.0), target(kmax + 1, 0.0);
+    for (int x = 0; x < ND2; ++x) {
+        const double m = (x == 0) ? 1.0 : 2.0;
+        const double ax2 = double(alfa[x]) * double(alfa[x]);
+        for (int z = 0; z < NE; ++z) {
+            const double gz = double(gamma[z]);
+            const double k = std::sqrt(ax2 + gz * gz);
+            const int sh = int(k + 0.5);
+            const std::complex<float> U1 = at(x, z, 0), U3 = at(x, z, 1);
+            const double e1 = double(U1.real()) * double(U1.real()) + double(U1.imag()) * double(U1.imag());
+            const double e3 = double(U3.real()) * double(U3.real()) + double(U3.imag()) * double(U3.imag());
+            if (k > 0.0 && k <= knyq && sh <= kmax) {
+                const int zh = (x == 0 && z > NED2) ? NE - z : z;
+                shell_e[sh] += m * (e1 + e3);
+                shell_w[sh] += m * (0.75 + 0.50 * hash01(x, zh, seed_init, 17));
+            }
+        }
+    }
+    const double k0 = std::max(1.0, double(K0));
+    for (int sh = 1; sh <= kmax; ++sh) {
+        const double k = double(sh);
+        target[sh] = (k < k0) ? std::pow(k / k0, 4) / (k0 * k0 * k0) : 1.0 / (k * k * k);
+        if (k < k0) {
+            const double low = k / k0;
+            target[sh] = (low * low * low * low) / (k0 * k0 * k0);
+        }
+    }
+    double e_orig = 0.0, e_tgt = 0.0;
+    for (int sh = 1; sh <= kmax; ++sh) {
+        e_orig += shell_e[sh];
+        e_tgt += target[sh];
+    }
+    if (e_orig > 0.0 && e_tgt > 0.0) {
+        const double norm = e_orig / e_tgt;
+        for (int x = 0; x < ND2; ++x) {
+            const double ax = double(alfa[x]), ax2 = ax * ax;
+            for (int z = 0; z < NE; ++z) {
+                const double gz = double(gamma[z]), gz2 = gz * gz;
+                const double k = std::sqrt(ax2 + gz2);
+                const int sh = int(k + 0.5);
+                if (k > 0.0 && k <= knyq && sh <= kmax && shell_w[sh] > 0.0) {
+                    int zh = z;
+                    double sgn = 1.0;
+                    if (x == 0 && z > NED2) {
+                        zh = NE - z;
+                        sgn = -1.0;
+                    }
+                    const double jit = 0.75 + 0.50 * hash01(x, zh, seed_init, 17);
+                    const double me = (norm * target[sh]) * jit / shell_w[sh];
+                    const double th = sgn * 2.0 * 3.14159265358979323846 * hash01(x, zh, seed_init, 53);
+                    const std::complex<float> ph(float(std::cos(th)), float(std::sin(th)));
+                    if (ax == 0.0) {
+                        at(x, z, 0) = float(std::sqrt(me)) * ph;
+                        at(x, z, 1) = std::complex<float>(0.0f, 0.0f);
+                    } else {
+                        const std::complex<float> w = float(std::sqrt(me / (1.0 + gz2 / ax2))) * ph;
+                        at(x, z, 0) = float(-gz / ax) * w;
+                        at(x, z, 1) = w;
+                    }
+                } else {
+                    at(x, z, 0) = at(x, z, 1) = std::complex<float>(0.0f, 0.0f);
+                }
+            }
+        }
+    }
+    // statistics block (cuda/pao_km3_cuda.cu:345-424)
+    double A[8] = {0, 0, 0, 0, 0, 0, 0, 0}, E110 = 0.0;
+    for (int x = 0; x < ND2; ++x) {
+        for (int z = 0; z < N; ++z) {
+            const double e1 = std::norm(at(x, z, 0)), e3 = std::norm(at(x, z, 1));
+            const double ax2 = double(alfa[x]) * double(alfa[x]);
+            const double gz2 = double(gamma[z]) * double(gamma[z]);
+            const double K2 = ax2 + gz2;
+            const double m = (x == 0) ? 1.0 : 2.0;
+            A[1] += m * e1;
+            A[2] += m * e3;
+            A[3] += m * e1 * ax2;
+            A[4] += m * e1 * gz2;
+            A[5] += m * e3 * ax2;
+            A[6] += m * e3 * gz2;
+            A[7] += m * (e1 + e3) * K2 * K2;
+            if (x == 0) E110 += e1;
+        }
+    }
+    const double Q2 = A[1] + A[2], W2 = A[3] + A[4] + A[5] + A[6];
+    const double visc = 1.0 / Re;
+    const double EP = visc * W2, De = 2.0 * visc * visc * A[7];
+    const double KOL = std::pow(visc * visc * visc / EP, 0.25);
+    if (stats) {
+        const double v[19] = {double(Re), Q2, W2, EP, 2.0 * A[1] / Q2 - 1.0, 2.0 * (A[3] + A[4]) / W2 - 1.0,
+                              0.5 * Q2 / EP, KOL, visc, DXZ / KOL, (E110 != 0.0) ? 2.0 * A[1] / E110 : 0.0,
+                              2.0 * PI / std::sqrt(2.0 * A[1] / A[3]), 2.0 * PI / std::sqrt(2.0 * A[1] / A[4]),
+                              2.0 * PI / std::sqrt(2.0 * A[2] / A[5]), 2.0 * PI / std::sqrt(2.0 * A[2] / A[6]),
+                              De, 0.5 * Q2 * De / (EP * EP), double(E1), double(E3)};
+        std::memcpy(stats, v, sizeof(v));
+    }
+    if (seed_out) *seed_out = seed;
+}
+
+}  // namespace
+
+extern "C" int dns2d_init_pao(dns2d_state *s, double *stats19, int *pao_seed)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    std::vector<std::complex<float>> uw;
+    pao_host(s->N, s->K0, s->Re, uw, stats19, pao_seed);
+    s->visc = float(1.0 / s->Re);
+    reset_scalars(s);
+    const size_t bytes = uw.size() * sizeof(std::complex<float>);
+    float2 *d_uw = nullptr;
+    // the compact velocity spectrum (2 N^2/2 complex) is staged in the phys buffer
+    if (bytes > 3 * (size_t)s->L * s->L * 4) return fail(s, DNS2D_ERR_NOMEM, "PAO staging");
+    d_uw = reinterpret_cast<float2 *>(s->phys);
+    DNS2D_CUDA(cudaMemcpyAsync(d_uw, uw.data(), bytes, cudaMemcpyHostToDevice, s->stream), "PAO upload");
+    s->ks->cols_init(s->ptrs(), d_uw, 0, s->stream);
+    DNS2D_LAUNCHED("cols_init(PAO)");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "PAO init");
+    s->initialised = true;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_init_vorticity(dns2d_state *s, const float *om2, const float *fnm1)
+{
+    if (!s || !om2) return DNS2D_ERR_ARG;
+    if (s->visc == 0.0f) s->visc = float(1.0 / s->Re);
+    reset_scalars(s);
+    int rc = upload_compact(s, om2, s->om2);
+    if (rc) return rc;
+    if (fnm1) {
+        rc = upload_compact(s, fnm1, s->fnm1);
+        if (rc) return rc;
+    } else {
+        DNS2D_CUDA(cudaMemsetAsync(s->fnm1, 0, (size_t)s->N * s->H * 8, s->stream), "fnm1 clear");
+    }
+    s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream);
+    DNS2D_LAUNCHED("cols_init(om2)");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "vorticity init");
+    s->initialised = true;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_k4_spectrum(int N, float K0, uint64_t seed, float *om2)
+{
+    if (!om2 || N < 8 || N % 8) return DNS2D_ERR_ARG;
+    const int H = N / 2;
+    std::vector<double> re((size_t)N * H), im((size_t)N * H);
+    uint64_t st = seed;
+    auto next = [&]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    };
+    const double k0 = K0;
+    for (int iz = 0; iz < N; ++iz)
+        for (int ix = 0; ix < H; ++ix) {
+            const double u = (double)(next() >> 11) * (1.0 / 9007199254740992.0);
+            const double th = 2.0 * M_PI * u;
+            const int kz = (iz < H) ? iz : iz - N;
+            const double k2 = (double)ix * ix + (double)kz * kz;
+            const size_t i = (size_t)iz * H + ix;
+            if (k2 == 0.0 || kz == -H) {
+                re[i] = im[i] = 0.0;
+                continue;
+            }
+            const double k = std::sqrt(k2), q = k / k0;
+            const double a = std::sqrt(k * q * q * q * q * std::exp(-2.0 * q * q));
+            re[i] = a * std::cos(th);
+            im[i] = a * std::sin(th);
+        }
+    for (int iz = H + 1; iz < N; ++iz) {  // Hermitian kx = 0 column
+        re[(size_t)iz * H] = re[(size_t)(N - iz) * H];
+        im[(size_t)iz * H] = -im[(size_t)(N - iz) * H];
+    }
+    double E = 0.0;
+    for (int iz = 0; iz < N; ++iz)
+        for (int ix = 0; ix < H; ++ix) {
+            const int kz = (iz < H) ? iz : iz - N;
+            const double k2 = (double)ix * ix + (double)kz * kz;
+            if (k2 == 0.0) continue;
+            const size_t i = (size_t)iz * H + ix;
+            E += 0.5 * (ix == 0 ? 1.0 : 2.0) * (re[i] * re[i] + im[i] * im[i]) / k2;
+        }
+    const double sc = (E > 0.0) ? std::sqrt(0.5 / E) : 0.0;
+    for (size_t i = 0; i < (size_t)N * H; ++i) {
+        om2[2 * i] = (float)(re[i] * sc);
+        om2[2 * i + 1] = (float)(im[i] * sc);
+    }
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_init_k4(dns2d_state *s, uint64_t seed)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    std::vector<float> om((size_t)s->N * s->H * 2);
+    int rc = dns2d_k4_spectrum(s->N, s->K0, seed, om.data());
+    if (rc) return rc;
+    return dns2d_init_vorticity(s, om.data(), nullptr);
+}
+
+// ============================================================================================
+// time stepping
+// ============================================================================================
+namespace {
+
+int get_graph(dns2d_state *s, int first, int K, cudaGraphExec_t *out)
+{
+    auto key = std::make_pair(first, K);
+    auto itg = s->graphs.find(key);
+    if (itg != s->graphs.end()) {
+        *out = itg->second;
+        return DNS2D_OK;
+    }
+    cudaGraph_t g = nullptr;
+    DNS2D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const Pointers p = s->ptrs();
+    for (int i = 0; i < K; ++i) {
+        s->ks->rows_step(p, s->stream);
+        s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream);
+    }
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess) return cuda_check(s, e, "end capture");
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_check(s, e, "graph instantiate");
+    s->graphs[key] = ex;
+    *out = ex;
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int dns2d_step(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist)
+{
+    if (!s || nsteps < 0) return DNS2D_ERR_ARG;
+    if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
+    int done = 0;
+    while (done < nsteps) {
+        const int K = std::min(kChunk, nsteps - done);
+        const int first = (done == 0) ? 1 : 0;
+        // parameters of this chunk: within a dns2d_step call dt is constant; after the first
+        // step of the call CNM1 == CN (cuda/step3_cuda.cu:172)
+        const float cnm1_first = (done == 0) ? s->cnm1 : s->cn;
+        k_set_params<<<1, 1, 0, s->stream>>>(s->prm, s->dt, cnm1_first, s->cn, s->visc);
+        DNS2D_LAUNCHED("set params");
+        if (s->timing) {
+            const Pointers p = s->ptrs();
+            for (int i = 0; i < K; ++i) {
+                phase_begin(s);
+                s->ks->rows_step(p, s->stream);
+                DNS2D_LAUNCHED("rows_step");
+                phase_end(s, 0);
+                phase_begin(s);
+                s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream);
+                DNS2D_LAUNCHED("cols_step");
+                phase_end(s, 1);
+            }
+        } else {
+            cudaGraphExec_t ex = nullptr;
+            int rc = get_graph(s, first, K, &ex);
+            if (rc) return rc;
+            DNS2D_CUDA(cudaGraphLaunch(ex, s->stream), "graph launch");
+        }
+        if (E_hist || Z_hist) {
+            DNS2D_CUDA(cudaMemcpyAsync(s->hist_host, s->hist, (size_t)K * 16, cudaMemcpyDeviceToHost, s->stream),
+                       "history copy");
+            DNS2D_CUDA(cudaStreamSynchronize(s->stream), "history sync");
+            for (int i = 0; i < K; ++i) {
+                if (E_hist) E_hist[done + i] = s->hist_host[i].x;
+                if (Z_hist) Z_hist[done + i] = s->hist_host[i].y;
+            }
+        }
+        // host scalars, step by step like the reference loop
+        for (int i = 0; i < K; ++i) {
+            s->it += 1;
+            const float dt_old = s->dt;
+            s->cnm1 = s->cn;
+            s->t += dt_old;
+        }
+        done += K;
+    }
+    return DNS2D_OK;
+}
+
+extern "C" void *dns2d_stream(dns2d_state *s) { return s ? (void *)s->stream : nullptr; }
+
+extern "C" int dns2d_sync(dns2d_state *s, int timeout_ms)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    if (timeout_ms <= 0) {
+        DNS2D_CUDA(cudaStreamSynchronize(s->stream), "sync");
+        return DNS2D_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaStreamQuery(s->stream);
+        if (e == cudaSuccess) return DNS2D_OK;
+        if (e != cudaErrorNotReady) return cuda_check(s, e, "sync");
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > timeout_ms) return fail(s, DNS2D_ERR_TIMEOUT, "device did not finish within %d ms", timeout_ms);
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+namespace {
+
+int compute_cflm(dns2d_state *s, float *out)
+{
+    const float PI = 3.14159265358979323846f;
+    const float DX = 2.0f * PI / float(s->N);
+    DNS2D_CUDA(cudaMemsetAsync(s->cflm_dev, 0, 4, s->stream), "cflm clear");
+    s->ks->rows_velocity(s->ptrs(), nullptr, s->cflm_dev, DX, s->stream);
+    DNS2D_LAUNCHED("rows_velocity(cfl)");
+    float h = 0.0f;
+    DNS2D_CUDA(cudaMemcpyAsync(&h, s->cflm_dev, 4, cudaMemcpyDeviceToHost, s->stream), "cflm copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "cflm sync");
+    *out = h;
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int dns2d_next_dt(dns2d_state *s, float *cflm_out)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
+    const float PI = 3.14159265358979323846f;
+    phase_begin(s);
+    float CFLM = 0.0f;
+    // NEXTDT init branch (cuda/dns_cuda.cu:562-569) and regular update (:572-579)
+    if (s->it == 0 && s->dt == 0.0f) {
+        int rc = compute_cflm(s, &CFLM);
+        if (rc) return rc;
+        s->dt = s->cflnum / CFLM / PI;
+        s->cflm = CFLM;
+    } else if (s->ifn > 0 && (s->it % s->ifn) == 0) {
+        int rc = compute_cflm(s, &CFLM);
+        if (rc) return rc;
+        const float CFL = CFLM * s->dt * PI;
+        s->cn = 0.8f + 0.2f * (s->cflnum / CFL);
+        s->dt = s->dt * s->cn;
+        s->cflm = CFLM;
+    }
+    phase_end(s, 2);
+    if (cflm_out) *cflm_out = s->cflm;
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// diagnostics
+// ============================================================================================
+extern "C" int dns2d_om2phys(dns2d_state *s)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    phase_begin(s);
+    const size_t plane = (size_t)s->L * s->L;
+    s->ks->cols_scalar(s->ptrs(), s->scratch, 0, s->stream);
+    DNS2D_LAUNCHED("cols_scalar");
+    s->ks->rows_scalar(s->ptrs(), s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
+    DNS2D_LAUNCHED("rows_scalar");
+    phase_end(s, 3);
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_stream_func(dns2d_state *s)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    const size_t plane = (size_t)s->L * s->L;
+    s->ks->cols_scalar(s->ptrs(), s->scratch, 1, s->stream);
+    DNS2D_LAUNCHED("cols_scalar(psi)");
+    s->ks->rows_scalar(s->ptrs(), s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
+    DNS2D_LAUNCHED("rows_scalar(psi)");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_velocity_phys(dns2d_state *s)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
+    s->ks->rows_velocity(s->ptrs(), s->phys, nullptr, 1.0f, s->stream);
+    DNS2D_LAUNCHED("rows_velocity(phys)");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_kinetic(dns2d_state *s)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    const size_t plane = (size_t)s->L * s->L;
+    k_kinetic<<<1024, 256, 0, s->stream>>>(s->phys, plane);
+    DNS2D_LAUNCHED("kinetic");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_display_sigma(dns2d_state *s, int comp, double *sigma)
+{
+    if (!s || !sigma || comp < 0 || comp > 2) return DNS2D_ERR_ARG;
+    phase_begin(s);
+    const size_t plane = (size_t)s->L * s->L;
+    const float *f = s->phys + (size_t)comp * plane;
+    const int nb = (int)std::min<size_t>(kSigmaBlocks, std::max<size_t>(1, (plane + 255) / 256));
+    k_minmax<<<nb, 256, 0, s->stream>>>(f, plane, s->minmax);
+    DNS2D_LAUNCHED("minmax");
+    std::vector<float2> mm((size_t)nb);
+    DNS2D_CUDA(cudaMemcpyAsync(mm.data(), s->minmax, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->stream), "minmax copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "minmax sync");
+    float minv = mm[0].x, maxv = mm[0].y;
+    for (int i = 1; i < nb; ++i) {
+        minv = std::min(minv, mm[(size_t)i].x);
+        maxv = std::max(maxv, mm[(size_t)i].y);
+    }
+    const float rng = maxv - minv;
+    const int is_constant = (std::fabs(rng) <= 1.0e-12f) ? 1 : 0;
+    k_sigma_pixels<<<nb, 256, 0, s->stream>>>(f, plane, minv, rng, is_constant, s->sums);
+    DNS2D_LAUNCHED("sigma pixels");
+    std::vector<unsigned long long> hs((size_t)nb * 2);
+    DNS2D_CUDA(cudaMemcpyAsync(hs.data(), s->sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, s->stream), "sums copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "sums sync");
+    unsigned long long a = 0, b = 0;
+    for (int i = 0; i < nb; ++i) {
+        a += hs[2 * (size_t)i];
+        b += hs[2 * (size_t)i + 1];
+    }
+    const double mean = (double)a / (double)plane;
+    const double var = std::max(0.0, (double)b / (double)plane - mean * mean);
+    *sigma = std::sqrt(var);
+    phase_end(s, 3);
+    return DNS2D_OK;
+}
+
+namespace {
+int om2_reduce(dns2d_state *s, double *v6)
+{
+    k_om2_reduce<<<kRedBlocks, 256, 0, s->stream>>>(s->om2, s->N, s->red);
+    DNS2D_LAUNCHED("om2 reduce");
+    std::vector<double> h((size_t)kRedBlocks * 6);
+    DNS2D_CUDA(cudaMemcpyAsync(h.data(), s->red, h.size() * 8, cudaMemcpyDeviceToHost, s->stream), "reduce copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "reduce sync");
+    for (int j = 0; j < 6; ++j) v6[j] = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b) {
+        for (int j = 0; j < 5; ++j) v6[j] += h[6 * (size_t)b + j];
+        v6[5] = std::max(v6[5], h[6 * (size_t)b + 5]);
+    }
+    return DNS2D_OK;
+}
+}  // namespace
+
+extern "C" int dns2d_energy_enstrophy(dns2d_state *s, double *E, double *Z)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    double v[6];
+    int rc = om2_reduce(s, v);
+    if (rc) return rc;
+    if (E) *E = v[0];
+    if (Z) *Z = v[1];
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_palin(dns2d_state *s, double *out)
+{
+    if (!s || !out) return DNS2D_ERR_ARG;
+    double v[6];
+    int rc = om2_reduce(s, v);
+    if (rc) return rc;
+    const double total = v[3] - v[4];
+    *out = (total <= 0.0 || v[5] <= 0.0) ? 0.0 : v[2] / (total * v[5]);
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_shell_spectrum(dns2d_state *s, double *Ek, int nb)
+{
+    if (!s || !Ek || nb <= 0) return DNS2D_ERR_ARG;
+    double *d = nullptr;
+    DNS2D_CUDA(cudaMallocAsync((void **)&d, (size_t)nb * 8, s->stream), "shell alloc");
+    DNS2D_CUDA(cudaMemsetAsync(d, 0, (size_t)nb * 8, s->stream), "shell clear");
+    k_shell<<<512, 256, 0, s->stream>>>(s->om2, s->N, d, nb);
+    DNS2D_LAUNCHED("shell");
+    DNS2D_CUDA(cudaMemcpyAsync(Ek, d, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->stream), "shell copy");
+    DNS2D_CUDA(cudaFreeAsync(d, s->stream), "shell free");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "shell sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_velocity_spectrum_bins(dns2d_state *s, double *esum, int *count, int nbins)
+{
+    if (!s || !esum || !count || nbins <= 0) return DNS2D_ERR_ARG;
+    double *d = nullptr;
+    int *c = nullptr;
+    DNS2D_CUDA(cudaMallocAsync((void **)&d, (size_t)nbins * 8, s->stream), "bins alloc");
+    DNS2D_CUDA(cudaMallocAsync((void **)&c, (size_t)nbins * 4, s->stream), "bins alloc");
+    DNS2D_CUDA(cudaMemsetAsync(d, 0, (size_t)nbins * 8, s->stream), "bins clear");
+    DNS2D_CUDA(cudaMemsetAsync(c, 0, (size_t)nbins * 4, s->stream), "bins clear");
+    k_vel_bins<<<1024, 256, 0, s->stream>>>(s->om2, s->N, d, c, nbins);
+    DNS2D_LAUNCHED("velocity bins");
+    DNS2D_CUDA(cudaMemcpyAsync(esum, d, (size_t)nbins * 8, cudaMemcpyDeviceToHost, s->stream), "bins copy");
+    DNS2D_CUDA(cudaMemcpyAsync(count, c, (size_t)nbins * 4, cudaMemcpyDeviceToHost, s->stream), "bins copy");
+    DNS2D_CUDA(cudaFreeAsync(d, s->stream), "bins free");
+    DNS2D_CUDA(cudaFreeAsync(c, s->stream), "bins free");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "bins sync");
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// state transfer
+// ============================================================================================
+extern "C" int dns2d_get_scalars(const dns2d_state *s, dns2d_scalars *o)
+{
+    if (!s || !o) return DNS2D_ERR_ARG;
+    o->N = s->N;
+    o->NX_full = s->L;
+    o->NK_full = s->Nk;
+    o->it = s->it;
+    o->ifn = s->ifn;
+    o->Re = s->Re;
+    o->K0 = s->K0;
+    o->visc = s->visc;
+    o->t = s->t;
+    o->dt = s->dt;
+    o->cn = s->cn;
+    o->cnm1 = s->cnm1;
+    o->cflnum = s->cflnum;
+    o->cflm = s->cflm;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_set_scalars(dns2d_state *s, const dns2d_scalars *i)
+{
+    if (!s || !i) return DNS2D_ERR_ARG;
+    if (i->N != s->N) return fail(s, DNS2D_ERR_ARG, "scalars for N=%d on a state of N=%d", i->N, s->N);
+    s->it = i->it;
+    s->ifn = i->ifn;
+    s->Re = i->Re;
+    s->K0 = i->K0;
+    s->visc = i->visc;
+    s->t = i->t;
+    s->dt = i->dt;
+    s->cn = i->cn;
+    s->cnm1 = i->cnm1;
+    s->cflnum = i->cflnum;
+    s->cflm = i->cflm;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_get_om2(dns2d_state *s, float *om2)
+{
+    if (!s || !om2) return DNS2D_ERR_ARG;
+    return download_compact(s, s->om2, om2);
+}
+
+extern "C" int dns2d_get_fnm1(dns2d_state *s, float *fnm1)
+{
+    if (!s || !fnm1) return DNS2D_ERR_ARG;
+    return download_compact(s, s->fnm1, fnm1);
+}
+
+extern "C" int dns2d_get_phys(dns2d_state *s, int comp, float *plane)
+{
+    if (!s || !plane || comp < 0 || comp > 2) return DNS2D_ERR_ARG;
+    const size_t n = (size_t)s->L * s->L;
+    DNS2D_CUDA(cudaMemcpyAsync(plane, s->phys + (size_t)comp * n, n * 4, cudaMemcpyDeviceToHost, s->stream), "phys copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "phys sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_set_velocity_phys(dns2d_state *s, const float *u, const float *w)
+{
+    if (!s || !u || !w) return DNS2D_ERR_ARG;
+    const size_t n = (size_t)s->L * s->L;
+    DNS2D_CUDA(cudaMemcpyAsync(s->phys, u, n * 4, cudaMemcpyHostToDevice, s->stream), "u upload");
+    DNS2D_CUDA(cudaMemcpyAsync(s->phys + n, w, n * 4, cudaMemcpyHostToDevice, s->stream), "w upload");
+    s->ks->rows_from_phys(s->ptrs(), s->phys, s->stream);
+    DNS2D_LAUNCHED("rows_from_phys");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "velocity upload");
+    s->initialised = true;
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// restart.bin (cuda/mem_cuda.cu:1019-1054 header, :1236-1394 writer/reader).
+// Little-endian, natural alignment: v1 header 136 bytes, v2 adds ur_full_count (144 bytes).
+// ============================================================================================
+namespace {
+
+#pragma pack(push, 4)
+struct RestartV1 {
+    char magic[16];
+    uint32_t version, header_bytes, real_bytes, cplx_bytes;
+    int32_t Nbase, N, NX, NZ, NK, NX_full, NZ_full, NK_full, it, ifn;
+    float Re, K0, visc, t, dt, cn, cnm1, cflnum, cflm;
+    uint32_t pad_;
+    uint64_t uc_full_count, om2_count, fnm1_count;
+};
+#pragma pack(pop)
+static_assert(sizeof(RestartV1) == 136, "restart v1 header size");
+struct RestartV2 {
+    RestartV1 v1;
+    uint64_t ur_full_count;
+};
+static_assert(sizeof(RestartV2) == 144, "restart v2 header size");
+
+}  // namespace
+
+extern "C" int dns2d_save_restart(dns2d_state *s, const char *path)
+{
+    if (!s || !path) return DNS2D_ERR_ARG;
+    const size_t n = (size_t)s->L * s->L, nom = (size_t)s->N * s->H;
+    RestartV2 h;
+    std::memset(&h, 0, sizeof(h));
+    std::snprintf(h.v1.magic, sizeof(h.v1.magic), "CTRB_RESTART");
+    h.v1.version = 2;
+    h.v1.header_bytes = sizeof(RestartV2);
+    h.v1.real_bytes = 4;
+    h.v1.cplx_bytes = 8;
+    h.v1.Nbase = h.v1.N = h.v1.NX = h.v1.NZ = s->N;
+    h.v1.NK = h.v1.NK_full = s->Nk;
+    h.v1.NX_full = h.v1.NZ_full = s->L;
+    h.v1.it = s->it;
+    h.v1.ifn = s->ifn;
+    h.v1.Re = s->Re;
+    h.v1.K0 = s->K0;
+    h.v1.visc = s->visc;
+    h.v1.t = s->t;
+    h.v1.dt = s->dt;
+    h.v1.cn = s->cn;
+    h.v1.cnm1 = s->cnm1;
+    h.v1.cflnum = s->cflnum;
+    h.v1.cflm = s->cflm;
+    h.v1.uc_full_count = 0;
+    h.v1.om2_count = h.v1.fnm1_count = nom;
+    h.ur_full_count = 3 * n;
+    int rc = dns2d_velocity_phys(s);
+    if (rc) return rc;
+    std::vector<float> buf(n);
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
+    bool ok = std::fwrite(&h, 1, sizeof(h), fp) == sizeof(h);
+    for (int c = 0; ok && c < 3; ++c) {
+        rc = dns2d_get_phys(s, c, buf.data());
+        if (rc) {
+            std::fclose(fp);
+            return rc;
+        }
+        ok = std::fwrite(buf.data(), 4, n, fp) == n;
+    }
+    std::vector<float> sp(nom * 2);
+    if (ok) {
+        rc = dns2d_get_om2(s, sp.data());
+        if (rc) {
+            std::fclose(fp);
+            return rc;
+        }
+        ok = std::fwrite(sp.data(), 8, nom, fp) == nom;
+    }
+    if (ok) {
+        rc = dns2d_get_fnm1(s, sp.data());
+        if (rc) {
+            std::fclose(fp);
+            return rc;
+        }
+        ok = std::fwrite(sp.data(), 8, nom, fp) == nom;
+    }
+    if (std::fclose(fp) != 0) ok = false;
+    return ok ? DNS2D_OK : fail(s, DNS2D_ERR_IO, "write failed: %s", path);
+}
+
+extern "C" int dns2d_load_restart(dns2d_state *s, const char *path)
+{
+    if (!s || !path) return DNS2D_ERR_ARG;
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
+    RestartV2 h;
+    std::memset(&h, 0, sizeof(h));
+    auto bad = [&](int code, const char *msg) {
+        std::fclose(fp);
+        return fail(s, code, "%s: %s", path, msg);
+    };
+    if (std::fread(&h.v1, 1, sizeof(h.v1), fp) != sizeof(h.v1)) return bad(DNS2D_ERR_IO, "short header");
+    if (std::strncmp(h.v1.magic, "CTRB_RESTART", 12) != 0) return bad(DNS2D_ERR_FORMAT, "bad magic");
+    if (h.v1.version == 2) {
+        if (h.v1.header_bytes != sizeof(RestartV2)) return bad(DNS2D_ERR_FORMAT, "header size");
+        if (std::fread(&h.ur_full_count, 1, 8, fp) != 8) return bad(DNS2D_ERR_IO, "short header");
+    }
+    if (h.v1.version < 1 || h.v1.version > 2 || (h.v1.version == 1 && h.v1.header_bytes != sizeof(RestartV1)) ||
+        h.v1.real_bytes != 4 || h.v1.cplx_bytes != 8)
+        return bad(DNS2D_ERR_FORMAT, "unsupported format");
+    if (h.v1.Nbase != s->N || h.v1.N != s->N || h.v1.NX != s->N || h.v1.NZ != s->N || h.v1.NK != s->Nk ||
+        h.v1.NX_full != s->L || h.v1.NZ_full != s->L || h.v1.NK_full != s->Nk)
+        return bad(DNS2D_ERR_FORMAT, "dimensions do not match this run");
+    const uint64_t ucn = (uint64_t)s->Nk * s->L * 3, urn = (uint64_t)s->L * s->L * 3, omn = (uint64_t)s->N * s->H;
+    const bool has_uc = h.v1.uc_full_count != 0;
+    if ((h.v1.version == 1 && h.v1.uc_full_count != ucn) || (h.v1.version >= 2 && has_uc && h.v1.uc_full_count != ucn) ||
+        (h.v1.version >= 2 && h.ur_full_count != urn) || h.v1.om2_count != omn || h.v1.fnm1_count != omn)
+        return bad(DNS2D_ERR_FORMAT, "array sizes do not match this run");
+    // UC_full payload (v1, or v2 with one) is skipped: the velocity is rebuilt from UR or OM2
+    if (h.v1.version == 1 || has_uc) {
+        if (std::fseek(fp, (long)(h.v1.uc_full_count * 8), SEEK_CUR) != 0) return bad(DNS2D_ERR_IO, "seek");
+    }
+    const size_t n = (size_t)s->L * s->L;
+    std::vector<float> u, w;
+    if (h.v1.version >= 2) {
+        u.resize(n);
+        w.resize(n);
+        if (std::fread(u.data(), 4, n, fp) != n || std::fread(w.data(), 4, n, fp) != n ||
+            std::fseek(fp, (long)(n * 4), SEEK_CUR) != 0)
+            return bad(DNS2D_ERR_IO, "short UR payload");
+    }
+    std::vector<float> om(omn * 2), fn(omn * 2);
+    if (std::fread(om.data(), 8, omn, fp) != omn || std::fread(fn.data(), 8, omn, fp) != omn)
+        return bad(DNS2D_ERR_IO, "short OM2/FNM1 payload");
+    std::fclose(fp);
+    int rc = upload_compact(s, om.data(), s->om2);
+    if (rc) return rc;
+    rc = upload_compact(s, fn.data(), s->fnm1);
+    if (rc) return rc;
+    if (h.v1.version >= 2) {
+        rc = dns2d_set_velocity_phys(s, u.data(), w.data());
+    } else {
+        s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream);  // velocity from OM2 (v1)
+        rc = cuda_check(s, cudaStreamSynchronize(s->stream), "v1 velocity");
+    }
+    if (rc) return rc;
+    s->Re = h.v1.Re;
+    s->K0 = h.v1.K0;
+    s->visc = h.v1.visc;
+    s->t = h.v1.t;
+    s->dt = h.v1.dt;
+    s->cn = h.v1.cn;
+    s->cnm1 = h.v1.cnm1;
+    s->cflnum = h.v1.cflnum;
+    s->cflm = h.v1.cflm;
+    s->it = h.v1.it;
+    s->ifn = h.v1.ifn;
+    s->initialised = true;
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// phase timing
+// ============================================================================================
+extern "C" int dns2d_phase_timing(dns2d_state *s, int enable)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    s->timing = enable != 0;
+    for (int i = 0; i < 4; ++i) {
+        s->phase_ms[i] = 0.0;
+        s->phase_n[i] = 0;
+    }
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_phase_report(dns2d_state *s, double *ms, long long *counts)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    for (int i = 0; i < 4; ++i) {
+        if (ms) ms[i] = s->phase_ms[i];
+        if (counts) counts[i] = s->phase_n[i];
+    }
+    return DNS2D_OK;
+}

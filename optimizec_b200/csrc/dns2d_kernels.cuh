@@ -1,0 +1,498 @@
+// dns2d_kernels.cuh — device kernels of the fused 2D vorticity step.
+//
+// Data layout in HBM (N base modes, L = 3N/2 padded grid, H = N/2 retained kx):
+//   om2, fnm1 : [kx][kz] complex64, kz in compact order iz (kz = iz < N/2 ? iz : iz - N).
+//               The reference keeps [iz][ix] (cuda/cuda_dns.h:62-63); the column pass reads
+//               whole kx columns, so the state is stored transposed here and converted at the
+//               API boundary.
+//   work      : [2][L/4][H][4] complex64.  Component c, physical row z, mode kx sits at
+//               ((z/4)*H + kx)*4 + z%4.  Between the column pass and the row pass it holds the
+//               velocity after the z-inverse transform, U(z,kx) and W(z,kx); between the row
+//               pass and the column pass it holds the x-forward transforms of the products,
+//               D(z,kx) = F_x[u^2 - w^2] and E(z,kx) = F_x[u w].  Groups of 4 rows are
+//               contiguous per kx, so the row pass reads/writes whole 4-row tiles and the column
+//               pass moves full 32-byte sectors.
+//
+// One time step of the reference (cuda/mem_cuda.cu:1848-1857: STEP2B -> STEP3 -> STEP2A)
+// becomes two kernels:
+//   row pass    (k_rows_step):  U,W rows -> C2R -> u,w -> (u+iw)^2 -> R2C -> D,E rows
+//               = STEP2A's x-inverse + STEP2B's products and x-forward
+//   column pass (k_cols_step):  D,E columns -> z-forward (kz in [-N/2,N/2)) -> FN ->
+//               Crank-Nicolson/AB2 update of om2, fnm1 <- FN -> velocity recovery ->
+//               3/2 zero-padding -> z-inverse -> U,W columns
+//               = STEP2B's z-forward + zero row N, STEP3, STEP2A's dealias/reshuffle/z-inverse
+#pragma once
+#include "fft.cuh"
+
+namespace dns2d {
+
+// ------------------------------------------------------------------------------------------
+// per-size configuration
+// ------------------------------------------------------------------------------------------
+template <int N_>
+struct Cfg;
+
+#define DNS2D_CFG(N_, ROWS_, NTB_, NTA_, ...)                                                  \
+    template <>                                                                                \
+    struct Cfg<N_> {                                                                           \
+        static constexpr int N = N_;                                                           \
+        static constexpr int H = N_ / 2;                                                       \
+        static constexpr int L = 3 * N_ / 2;                                                   \
+        static constexpr int LP = SmemLen<L>::value;                                           \
+        static constexpr int ROWS = ROWS_;                                                     \
+        static constexpr int NTB = NTB_;                                                       \
+        static constexpr int NTA = NTA_;                                                       \
+        using Plan = Radices<__VA_ARGS__>;                                                     \
+    };
+
+//          N     ROWS  NTB  NTA  radix plan (product = 3N/2)
+DNS2D_CFG(16,    4,   64,  32,  4, 6)
+DNS2D_CFG(32,    4,   64,  32,  8, 6)
+DNS2D_CFG(64,    4,  128,  64,  8, 12)
+DNS2D_CFG(128,   4,  192,  64,  16, 12)
+DNS2D_CFG(256,   4,  256, 128,  16, 24)
+DNS2D_CFG(512,   4,  384, 192,  16, 16, 3)
+DNS2D_CFG(1024,  4,  512, 256,  16, 8, 12)
+DNS2D_CFG(2048,  4,  768, 384,  16, 16, 12)
+DNS2D_CFG(4096,  2,  768, 768,  16, 16, 24)
+#undef DNS2D_CFG
+
+// work-buffer index (float2 units) of component c, physical row z, mode kx
+template <int L, int H>
+__device__ __forceinline__ size_t widx(int c, int z, int kx)
+{
+    return (size_t)c * ((size_t)L * H) + (((size_t)(z >> 2) * H + kx) << 2) + (z & 3);
+}
+
+// parameters that change between segments of the run (read from device memory so a captured
+// CUDA graph can be replayed with new values)
+struct StepParams {
+    float dt;          // time step of this segment
+    float cnm1_first;  // CNM1 seen by the first step of the segment (host value before it)
+    float cn;          // CN; after the first step the reference has CNM1 == CN
+    float visc;        // viscosity
+};
+
+struct Pointers {
+    float2 *om2;
+    float2 *fnm1;
+    float2 *work;
+    const float2 *tw;       // W_L^j, j in [0, L)
+    const StepParams *prm;
+    double2 *part;          // per-column (E, Z) partial sums, [H]
+    unsigned int *counter;  // arrival counter for the last-block reduction
+    double2 *hist;          // per-step (E, Z) history
+};
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+
+// CFL contribution |u|/DX + |w|/DZ with IEEE division/addition (cuda/dns_cuda.cu:497-502)
+__device__ __forceinline__ float cfl_term(float u, float w, float dx)
+{
+    return __fadd_rn(__fdiv_rn(fabsf(u), dx), __fdiv_rn(fabsf(w), dx));
+}
+
+// ordered max of non-negative floats through their bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(float *addr, float v)
+{
+    atomicMax(reinterpret_cast<unsigned int *>(addr), __float_as_uint(v));
+}
+
+template <int NT>
+__device__ __forceinline__ float block_max(float v, float *red)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < (NT + 31) / 32) ? red[l] : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;  // valid in thread 0
+}
+
+template <int NT>
+__device__ __forceinline__ double2 block_sum2(double2 v, double2 *red)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = (l < (NT + 31) / 32) ? red[l] : make_double2(0.0, 0.0);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+    }
+    return v;  // valid in thread 0
+}
+
+// Hermitian packing of two real rows' half spectra a = F[u], b = F[w] (kx < H) into the full
+// complex spectrum of u + i w.  Like a C2R transform, only Re of the kx = 0 entries is used.
+template <int L, int H, int ROWS, int NT, int LP>
+__device__ __forceinline__ void rows_load_pack(float2 *s, const float2 *__restrict__ work, int z0)
+{
+    for (int e = threadIdx.x; e < ROWS * H; e += NT) {
+        const int r = e % ROWS, k = e / ROWS;
+        const float2 a = work[widx<L, H>(0, z0 + r, k)];
+        const float2 b = work[widx<L, H>(1, z0 + r, k)];
+        float2 *x = s + r * LP;
+        if (k == 0) {
+            x[sidx(0)] = make_float2(a.x, b.x);
+        } else {
+            x[sidx(k)] = make_float2(a.x - b.y, a.y + b.x);
+            x[sidx(L - k)] = make_float2(a.x + b.y, b.x - a.y);
+        }
+    }
+    constexpr int NZ = L - 2 * H + 1;  // zero band kx in [H, L-H]
+    for (int e = threadIdx.x; e < ROWS * NZ; e += NT) {
+        const int r = e / NZ, k = H + (e - r * NZ);
+        s[r * LP + sidx(k)] = make_float2(0.f, 0.f);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Row pass of one step.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    extern __shared__ float2 smem[];
+    const int z0 = blockIdx.x * ROWS;
+    rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
+    __syncthreads();
+    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    // products: (u + i w)^2 = (u^2 - w^2) + i (2 u w)
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        float2 *a = smem + r * LP + sidx(x);
+        const float2 z = *a;
+        *a = make_float2(z.x * z.x - z.y * z.y, 2.0f * z.x * z.y);
+    }
+    __syncthreads();
+    fft_run<L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    // unpack: D = F[u^2 - w^2] = (Q[k] + conj Q[L-k]) / 2, E = F[u w] = -i (Q[k] - conj Q[L-k]) / 4
+    for (int e = threadIdx.x; e < ROWS * H; e += NT) {
+        const int r = e % ROWS, k = e / ROWS;
+        const float2 *x = smem + r * LP;
+        const float2 q = x[sidx(k)];
+        const float2 m = x[sidx(k == 0 ? 0 : L - k)];
+        p.work[widx<L, H>(0, z0 + r, k)] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
+        p.work[widx<L, H>(1, z0 + r, k)] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Velocity recovery of one mode (cuda/step3_cuda.cu:103-138): u = -i kz om / K^2,
+// w = i kx om / K^2; on kx = 0: u = -i om / kz (0 at kz = 0), w = 0.  The factors kz/K^2 and
+// kx/K^2 are formed in FP64 and rounded once.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void recover_velocity(int kx, int kz, float2 om, float2 &u, float2 &w,
+                                                 double &invK2)
+{
+    const double K2 = (double)kx * kx + (double)kz * kz;
+    invK2 = (K2 > 0.0) ? 1.0 / K2 : 0.0;
+    float gu, gw;
+    if (kx >= 1) {
+        gu = (float)((double)kz * invK2);
+        gw = (float)((double)kx * invK2);
+    } else {
+        gu = (kz != 0) ? (float)(1.0 / (double)kz) : 0.0f;
+        gw = 0.0f;
+    }
+    // -i * gu * om = (gu*om.y, -gu*om.x); +i * gw * om = (-gw*om.y, gw*om.x)
+    u = make_float2(gu * om.y, -gu * om.x);
+    w = make_float2(-gw * om.y, gw * om.x);
+}
+
+// ------------------------------------------------------------------------------------------
+// Column pass of one step.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p, int first, int hist_slot)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
+    extern __shared__ float2 smem[];
+    __shared__ double2 red[32];
+    __shared__ bool am_last;
+    const int kx = blockIdx.x;
+    float2 *sD = smem, *sE = smem + LP;
+    for (int z = threadIdx.x; z < L; z += NT) {
+        sD[sidx(z)] = p.work[widx<L, H>(0, z, kx)];
+        sE[sidx(z)] = p.work[widx<L, H>(1, z, kx)];
+    }
+    __syncthreads();
+    fft_run<L, LP, false, 2, NT>(smem, p.tw, typename C::Plan{});
+
+    const StepParams prm = *p.prm;
+    const float dt = prm.dt;
+    const float cnm1 = first ? prm.cnm1_first : prm.cn;
+    // Crank-Nicolson factors in FP64: om' = ((1-a) om + dt/2 (2+cnm1) FN - dt/2 cnm1 FNM1)/(1+a)
+    const double hvdt = 0.5 * (double)prm.visc * (double)dt;
+    const double c2n = 0.5 * (double)dt * (2.0 + (double)cnm1);
+    const double c3n = -0.5 * (double)dt * (double)cnm1;
+    const float divxz = (float)(1.0 / ((double)L * (double)L));
+    double2 ez = make_double2(0.0, 0.0);
+    const double wgt = (kx == 0) ? 0.5 : 1.0;  // 1/2 * (1 on kx = 0, else 2)
+    float2 *om2c = p.om2 + (size_t)kx * N;
+    float2 *fnc = p.fnm1 + (size_t)kx * N;
+    for (int iz = threadIdx.x; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        const float2 d = sD[sidx(kzi)];
+        const float2 e = sE[sidx(kzi)];
+        float2 fn = make_float2(0.f, 0.f);
+        if (kz != -H) {  // STEP2B zeroes the kz = -N/2 row (cuda/step2b_cuda.cu:203-221)
+            const float ga = (float)kz * (float)kx;
+            const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
+            fn.x = (ga * d.x + g2a2 * e.x) * divxz;
+            fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+        }
+        const double K2 = (double)kx * kx + (double)kz * kz;
+        const double arg = hvdt * K2;
+        const double inv = 1.0 / (1.0 + arg);
+        const float c1 = (float)((1.0 - arg) * inv);
+        const float c2 = (float)(c2n * inv);
+        const float c3 = (float)(c3n * inv);
+        const float2 om = om2c[iz];
+        const float2 fo = fnc[iz];
+        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        om2c[iz] = on;
+        fnc[iz] = fn;
+        float2 u, w;
+        double invK2;
+        recover_velocity(kx, kz, on, u, w, invK2);
+        sD[sidx(kzi)] = u;
+        sE[sidx(kzi)] = w;
+        const double pw = (double)on.x * on.x + (double)on.y * on.y;
+        ez.x += wgt * pw * invK2;
+        ez.y += wgt * pw;
+    }
+    for (int z = H + threadIdx.x; z < L - H; z += NT) {  // 3/2 zero padding in kz
+        sD[sidx(z)] = make_float2(0.f, 0.f);
+        sE[sidx(z)] = make_float2(0.f, 0.f);
+    }
+    // energy / enstrophy of the updated field: per-column partials, the last block sums them
+    // in column order (deterministic)
+    ez = block_sum2<NT>(ez, red);
+    if (threadIdx.x == 0) {
+        p.part[kx] = ez;
+        __threadfence();
+        const unsigned int n = atomicAdd(p.counter, 1u);
+        am_last = (n == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (am_last) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int i = threadIdx.x; i < H; i += NT) {
+            const double2 q = __ldcg(&p.part[i]);
+            acc.x += q.x;
+            acc.y += q.y;
+        }
+        acc = block_sum2<NT>(acc, red);
+        if (threadIdx.x == 0) {
+            p.hist[hist_slot] = acc;
+            *p.counter = 0u;
+        }
+    }
+    __syncthreads();
+    fft_run<L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) {
+        p.work[widx<L, H>(0, z, kx)] = sD[sidx(z)];
+        p.work[widx<L, H>(1, z, kx)] = sE[sidx(z)];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Column set-up: velocity spectrum -> U, W columns.
+// mode 0: from the compact velocity spectrum uw[iz][ix][2] (PAO); om2 = i (kz u - kx w)
+//         (CALCOM, cuda/calcom_cuda.cu:117-131), fnm1 = 0.
+// mode 1: from om2 (already in [kx][kz] layout): velocity recovery; om2/fnm1 left unchanged.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p, const float2 *__restrict__ uw,
+                                                           int mode)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
+    extern __shared__ float2 smem[];
+    const int kx = blockIdx.x;
+    float2 *sU = smem, *sW = smem + LP;
+    for (int iz = threadIdx.x; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        float2 u, w;
+        if (mode == 0) {
+            const size_t b = 2 * ((size_t)iz * H + kx);
+            u = uw[b];
+            w = uw[b + 1];
+            const float gz = (float)kz, ax = (float)kx;
+            const float dx_ = gz * u.x - ax * w.x, dy_ = gz * u.y - ax * w.y;
+            p.om2[(size_t)kx * N + iz] = make_float2(-dy_, dx_);
+            p.fnm1[(size_t)kx * N + iz] = make_float2(0.f, 0.f);
+        } else {
+            double invK2;
+            recover_velocity(kx, kz, p.om2[(size_t)kx * N + iz], u, w, invK2);
+        }
+        sU[sidx(kzi)] = u;
+        sW[sidx(kzi)] = w;
+    }
+    for (int z = H + threadIdx.x; z < L - H; z += NT) {
+        sU[sidx(z)] = make_float2(0.f, 0.f);
+        sW[sidx(z)] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_run<L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) {
+        p.work[widx<L, H>(0, z, kx)] = sU[sidx(z)];
+        p.work[widx<L, H>(1, z, kx)] = sW[sidx(z)];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Velocity rows: U,W rows -> u,w physical (STEP2A's x-inverse).  Optionally writes u, w into
+// phys[0], phys[1] ([L][L] float each) and/or reduces the CFL maximum (NEXTDT, DX = 2 pi / N).
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p, float *phys, float *cflm,
+                                                               float dx)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    extern __shared__ float2 smem[];
+    __shared__ float red[32];
+    const int z0 = blockIdx.x * ROWS;
+    rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
+    __syncthreads();
+    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    float m = 0.0f;
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        const float2 z = smem[r * LP + sidx(x)];
+        if (phys) {
+            const size_t o = (size_t)(z0 + r) * L + x;
+            phys[o] = z.x;
+            phys[(size_t)L * L + o] = z.y;
+        }
+        m = fmaxf(m, cfl_term(z.x, z.y, dx));
+    }
+    if (cflm) {
+        m = block_max<NT>(m, red);
+        if (threadIdx.x == 0) atomic_max_nonneg(cflm, m);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Physical rows -> U,W rows (x-forward of u, w scaled by 1/L): loading a restart file's UR.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_from_phys(Pointers p, const float *phys)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    extern __shared__ float2 smem[];
+    const int z0 = blockIdx.x * ROWS;
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        const size_t o = (size_t)(z0 + r) * L + x;
+        smem[r * LP + sidx(x)] = make_float2(phys[o], phys[(size_t)L * L + o]);
+    }
+    __syncthreads();
+    fft_run<L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    const float sc = 1.0f / (float)L;
+    for (int e = threadIdx.x; e < ROWS * H; e += NT) {
+        const int r = e % ROWS, k = e / ROWS;
+        const float2 *x = smem + r * LP;
+        const float2 q = x[sidx(k)];
+        const float2 m = x[sidx(k == 0 ? 0 : L - k)];
+        p.work[widx<L, H>(0, z0 + r, k)] = make_float2(0.5f * sc * (q.x + m.x), 0.5f * sc * (q.y - m.y));
+        p.work[widx<L, H>(1, z0 + r, k)] = make_float2(0.5f * sc * (q.y + m.y), -0.5f * sc * (q.x - m.x));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Scalar field to physical space (OM2PHYS, stream function): one compact spectrum column ->
+// z-inverse -> scratch (component 0 of a work-shaped buffer).  kind 0: om2; kind 1: om2/K^2
+// with the (0,0) mode zeroed (cuda/om2phys_cuda.cu:232-256).
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_scalar(Pointers p, float2 *scratch, int kind)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
+    extern __shared__ float2 smem[];
+    const int kx = blockIdx.x;
+    for (int iz = threadIdx.x; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        float2 v = p.om2[(size_t)kx * N + iz];
+        if (kind == 1) {
+            const float k2 = (float)kx * (float)kx + (float)kz * (float)kz + 1.0e-30f;
+            v = make_float2(v.x / k2, v.y / k2);
+            if (kx == 0 && iz == 0) v = make_float2(0.f, 0.f);
+        }
+        smem[sidx(kzi)] = v;
+    }
+    for (int z = H + threadIdx.x; z < L - H; z += NT) smem[sidx(z)] = make_float2(0.f, 0.f);
+    __syncthreads();
+    fft_run<L, LP, true, 1, NT>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) scratch[widx<L, H>(0, z, kx)] = smem[sidx(z)];
+}
+
+// scratch rows -> real field rows written to out ([L][L]); per-block min/max partials
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_scalar(Pointers p, const float2 *scratch, float *out,
+                                                             float2 *minmax)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    extern __shared__ float2 smem[];
+    __shared__ float red[32];
+    const int z0 = blockIdx.x * ROWS;
+    for (int e = threadIdx.x; e < ROWS * H; e += NT) {
+        const int r = e % ROWS, k = e / ROWS;
+        const float2 a = scratch[widx<L, H>(0, z0 + r, k)];
+        float2 *x = smem + r * LP;
+        if (k == 0) {
+            x[sidx(0)] = make_float2(a.x, 0.f);
+        } else {
+            x[sidx(k)] = a;
+            x[sidx(L - k)] = make_float2(a.x, -a.y);
+        }
+    }
+    constexpr int NZ = L - 2 * H + 1;
+    for (int e = threadIdx.x; e < ROWS * NZ; e += NT) {
+        const int r = e / NZ, k = H + (e - r * NZ);
+        smem[r * LP + sidx(k)] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    float mn = 3.402823466e38f, mx = -3.402823466e38f;
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        const float v = smem[r * LP + sidx(x)].x;
+        out[(size_t)(z0 + r) * L + x] = v;
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+    // block min/max (max of -min)
+    __shared__ float s_nmn;
+    const float nmn = block_max<NT>(-mn, red);
+    if (threadIdx.x == 0) s_nmn = nmn;
+    const float bmx = block_max<NT>(mx, red);
+    if (threadIdx.x == 0) minmax[blockIdx.x] = make_float2(-s_nmn, bmx);
+}
+
+}  // namespace dns2d
