@@ -116,6 +116,25 @@ int dns2d_set_velocity_phys(dns2d_state *s, const float *u, const float *w);
 int dns2d_save_restart(dns2d_state *s, const char *path);
 int dns2d_load_restart(dns2d_state *s, const char *path);
 
+/* ---- time step without device allocation (no counterpart in the reference) ----
+ * For callers that cannot allocate device memory: an application that hands out only its own
+ * pooled or arena buffers, a process under a fixed device-memory budget, or code where
+ * cudaMalloc is not allowed.  The caller passes the state in its own device buffers:
+ *   om2, fnm1  device arrays [iz][ix] complex64 (N rows of N/2), advanced nsteps steps in place
+ *   visc, dt   viscosity and time step; cnm1 is used by the first step, cn by the later ones
+ *              (the reference's CNM1 <- CN rule); stream is a cudaStream_t (NULL = default)
+ * Nothing is allocated: all scratch (about 20 N^2 bytes) lives in one static device array of
+ * DNS2D_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the process exits,
+ * which limits N to DNS2D_NOALLOC_MAX_N; larger N returns DNS2D_ERR_SIZE.  The first call on a
+ * device looks up that array's device address (with the device current), so make the first call
+ * before any stream capture.  Every call shares the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  The call is asynchronous
+ * on the stream; the host scalars (t, it, cnm1) are the caller's to advance. */
+#define DNS2D_NOALLOC_MAX_N 512
+#define DNS2D_NOALLOC_SCRATCH_BYTES (6u << 20)
+int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float cn, int nsteps,
+                       void *om2, void *fnm1, void *stream);
+
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);
 /* ms[0..3], counts[0..3]: row pass, column pass, NEXTDT/CFLM, OM2PHYS+sigma */

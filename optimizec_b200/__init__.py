@@ -35,7 +35,7 @@ SYMBOLS = [
     "dns2d_energy_enstrophy", "dns2d_shell_spectrum", "dns2d_palin",
     "dns2d_velocity_spectrum_bins", "dns2d_get_scalars", "dns2d_set_scalars", "dns2d_get_om2",
     "dns2d_get_fnm1", "dns2d_get_phys", "dns2d_set_velocity_phys", "dns2d_save_restart",
-    "dns2d_load_restart", "dns2d_phase_timing", "dns2d_phase_report",
+    "dns2d_load_restart", "dns2d_phase_timing", "dns2d_phase_report", "dns2d_step_noalloc",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -121,6 +121,8 @@ def lib():
         "dns2d_load_restart": (C.c_int, [vp, C.c_char_p]),
         "dns2d_phase_timing": (C.c_int, [vp, C.c_int]),
         "dns2d_phase_report": (C.c_int, [vp, dp, C.POINTER(C.c_longlong)]),
+        "dns2d_step_noalloc": (C.c_int, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                         vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

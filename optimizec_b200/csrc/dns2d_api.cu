@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1387,4 +1388,112 @@ extern "C" int dns2d_phase_report(dns2d_state *s, double *ms, long long *counts)
         if (counts) counts[i] = s->phase_n[i];
     }
     return DNS2D_OK;
+}
+
+// ============================================================================================
+// Time step without device allocation.
+//
+// For callers that may not allocate device memory at all (an application that hands the solver
+// fixed buffers from its own pool or arena, a process under a strict device-memory budget, or
+// code running where cudaMalloc is forbidden).  The caller owns the vorticity state; everything
+// else the step needs (the U,W / D,E work buffer, transposed copies of the state, twiddles,
+// parameter block, reduction partials) lives in one static device array of this file.
+// ============================================================================================
+namespace {
+
+// one array per device, allocated when the module loads and held until the process exits
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DNS2D_NOALLOC_SCRATCH_BYTES];
+
+// per-device address of g_noalloc_scratch, looked up once per device with that device current
+unsigned char *noalloc_scratch_address(int *err)
+{
+    static std::mutex mu;
+    static unsigned char *addr[128] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 128) {
+        *err = DNS2D_ERR_CUDA;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            *err = DNS2D_ERR_CUDA;
+            return nullptr;
+        }
+        addr[dev] = static_cast<unsigned char *>(p);
+    }
+    return addr[dev];
+}
+
+// W_L^j built in FP64 and rounded once, on the device
+__global__ void k_noalloc_twiddles(float2 *tw, int L)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < L; j += gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)j / (double)L, &sn, &cs);
+        tw[j] = make_float2((float)cs, (float)-sn);
+    }
+}
+
+__global__ void k_noalloc_reset(unsigned int *counter) { *counter = 0u; }
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float cn, int nsteps,
+                                  void *om2, void *fnm1, void *stream)
+{
+    if (N > DNS2D_NOALLOC_MAX_N) return DNS2D_ERR_SIZE;
+    const KernelSet *ks = kernel_set(N);
+    if (!ks) return DNS2D_ERR_SIZE;
+    if (!om2 || !fnm1 || nsteps < 0) return DNS2D_ERR_ARG;
+    const size_t H = N / 2, L = 3 * (size_t)N / 2, nom = (size_t)N * H;
+    // scratch layout inside g_noalloc_scratch
+    const size_t o_work = 0;
+    const size_t o_om = o_work + align256(2 * L * H * sizeof(float2));
+    const size_t o_fn = o_om + align256(nom * sizeof(float2));
+    const size_t o_tw = o_fn + align256(nom * sizeof(float2));
+    const size_t o_prm = o_tw + align256(L * sizeof(float2));
+    const size_t o_part = o_prm + align256(sizeof(StepParams));
+    const size_t o_cnt = o_part + align256(H * sizeof(double2));
+    const size_t o_hist = o_cnt + align256(sizeof(unsigned int));
+    const size_t total = o_hist + align256(sizeof(double2));
+    if (total > DNS2D_NOALLOC_SCRATCH_BYTES) return DNS2D_ERR_SIZE;
+    int err = DNS2D_OK;
+    unsigned char *base = noalloc_scratch_address(&err);
+    if (!base) return err;
+    if (ks->setup() != cudaSuccess) return DNS2D_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Pointers p;
+    p.work = reinterpret_cast<float2 *>(base + o_work);
+    p.om2 = reinterpret_cast<float2 *>(base + o_om);
+    p.fnm1 = reinterpret_cast<float2 *>(base + o_fn);
+    p.tw = reinterpret_cast<const float2 *>(base + o_tw);
+    p.prm = reinterpret_cast<const StepParams *>(base + o_prm);
+    p.part = reinterpret_cast<double2 *>(base + o_part);
+    p.counter = reinterpret_cast<unsigned int *>(base + o_cnt);
+    p.hist = reinterpret_cast<double2 *>(base + o_hist);
+    // the array keeps the previous call's contents: rebuild twiddles, parameters and counter
+    k_noalloc_twiddles<<<(unsigned)((L + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(base + o_tw), (int)L);
+    k_set_params<<<1, 1, 0, st>>>(reinterpret_cast<StepParams *>(base + o_prm), dt, cnm1, cn, visc);
+    k_noalloc_reset<<<1, 1, 0, st>>>(p.counter);
+    dim3 tb(32, 8);
+    k_transpose_c64<<<dim3((unsigned)((H + 31) / 32), (unsigned)((N + 31) / 32)), tb, 0, st>>>(
+        static_cast<const float2 *>(om2), p.om2, N, (int)H);
+    k_transpose_c64<<<dim3((unsigned)((H + 31) / 32), (unsigned)((N + 31) / 32)), tb, 0, st>>>(
+        static_cast<const float2 *>(fnm1), p.fnm1, N, (int)H);
+    ks->cols_init(p, nullptr, 1, st);  // velocity of the given vorticity
+    for (int i = 0; i < nsteps; ++i) {
+        ks->rows_step(p, st);
+        ks->cols_step(p, i == 0 ? 1 : 0, 0, st);
+    }
+    k_transpose_c64<<<dim3((unsigned)((N + 31) / 32), (unsigned)((H + 31) / 32)), tb, 0, st>>>(
+        p.om2, static_cast<float2 *>(om2), (int)H, N);
+    k_transpose_c64<<<dim3((unsigned)((N + 31) / 32), (unsigned)((H + 31) / 32)), tb, 0, st>>>(
+        p.fnm1, static_cast<float2 *>(fnm1), (int)H, N);
+    return cudaGetLastError() == cudaSuccess ? DNS2D_OK : DNS2D_ERR_CUDA;
 }
