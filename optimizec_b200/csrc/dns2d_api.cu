@@ -33,6 +33,7 @@ namespace {
 struct KernelSet {
     int N;
     int rows_blocks;
+    const TwCatalog *cat;
     cudaError_t (*setup)();
     void (*rows_step)(const Pointers &, cudaStream_t);
     void (*cols_step)(const Pointers &, int, int, cudaStream_t);
@@ -51,10 +52,17 @@ struct Launch {
     static constexpr size_t smA1 = (size_t)C::LP * sizeof(float2);
     static constexpr int GB = C::L / C::ROWS;
 
+    static constexpr bool V2 = Cfg2<N>::enabled;
+    static constexpr size_t sm2 = V2 ? (size_t)SmemLen<3 * N / 2>::value * sizeof(float2) : 0;
+
     static cudaError_t setup()
     {
         const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
         cudaError_t e;
+        if constexpr (V2) {
+            if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
+        }
         if ((e = cudaFuncSetAttribute(k_rows_step<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_init<N>, a, (int)smA)) != cudaSuccess) return e;
@@ -64,10 +72,15 @@ struct Launch {
         if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
         return cudaSuccess;
     }
-    static void rows_step(const Pointers &p, cudaStream_t s) { k_rows_step<N><<<GB, C::NTB, smB, s>>>(p); }
+    static void rows_step(const Pointers &p, cudaStream_t s)
+    {
+        if constexpr (V2) k_rows_step2<N><<<C::L, Cfg2<N>::NT, sm2, s>>>(p);
+        else k_rows_step<N><<<GB, C::NTB, smB, s>>>(p);
+    }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s)
     {
-        k_cols_step<N><<<C::H, C::NTA, smA, s>>>(p, first, slot);
+        if constexpr (V2) k_cols_step2<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        else k_cols_step<N><<<C::H, C::NTA, smA, s>>>(p, first, slot);
     }
     static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s)
     {
@@ -91,8 +104,8 @@ struct Launch {
     }
     static KernelSet make()
     {
-        return KernelSet{N, GB, setup, rows_step, cols_step, cols_init, rows_velocity, rows_from_phys,
-                         cols_scalar, rows_scalar};
+        return KernelSet{N, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
+                         rows_from_phys, cols_scalar, rows_scalar};
     }
 };
 
@@ -381,14 +394,19 @@ void free_graphs(dns2d_state *s)
     s->graphs.clear();
 }
 
-// twiddle table W_L^j = exp(-2 pi i j/L) built in FP64 and rounded once
-std::vector<float2> twiddles(int L)
+// per-stage twiddle tables of a catalog: entry off + (r-1) Ns + k = W_{Ns R}^{r k}, built in
+// FP64 from the exactly reduced fraction (r k mod Ns R) / (Ns R) and rounded once
+std::vector<float2> twiddles(const TwCatalog &c)
 {
-    std::vector<float2> t((size_t)L);
-    for (int j = 0; j < L; ++j) {
-        // exact symmetric reduction of the angle to the first octant-free form
-        const double a = 2.0 * M_PI * (double)j / (double)L;
-        t[(size_t)j] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    std::vector<float2> t((size_t)std::max(c.total, 1));
+    for (int i = 0; i < c.n; ++i) {
+        const int R = c.R[i], NS = c.NS[i], M = R * NS;
+        for (int r = 1; r < R; ++r)
+            for (int k = 0; k < NS; ++k) {
+                const long long m = ((long long)r * k) % M;
+                const double a = 2.0 * M_PI * (double)m / (double)M;
+                t[(size_t)c.off[i] + (size_t)(r - 1) * NS + k] = make_float2((float)std::cos(a), (float)-std::sin(a));
+            }
     }
     return t;
 }
@@ -441,7 +459,7 @@ extern "C" size_t dns2d_device_bytes(int N)
            + 2 * L * H * 8            // work
            + L * H * 8                // scratch
            + 3 * L * L * 4            // phys
-           + L * 8 + H * 16 + kHistCap * 16;
+           + 2 * L * 8 + H * 16 + kHistCap * 16;
 }
 
 extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float cflnum, int device)
@@ -473,7 +491,7 @@ extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float 
     auto dalloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
     if (!dalloc((void **)&s->om2, nom * 8) || !dalloc((void **)&s->fnm1, nom * 8) ||
         !dalloc((void **)&s->work, 2 * L * H * 8) || !dalloc((void **)&s->scratch, L * H * 8) ||
-        !dalloc((void **)&s->phys, 3 * L * L * 4) || !dalloc((void **)&s->tw, L * 8) ||
+        !dalloc((void **)&s->phys, 3 * L * L * 4) || !dalloc((void **)&s->tw, (size_t)std::max(ks->cat->total, 1) * 8) ||
         !dalloc((void **)&s->prm, sizeof(StepParams)) || !dalloc((void **)&s->part, H * 16) ||
         !dalloc((void **)&s->hist, (size_t)kHistCap * 16) || !dalloc((void **)&s->counter, 4) ||
         !dalloc((void **)&s->cflm_dev, 4) || !dalloc((void **)&s->minmax, (size_t)std::max(kSigmaBlocks, ks->rows_blocks) * 8) ||
@@ -483,8 +501,8 @@ extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float 
     }
     s->hist_cap = kHistCap;
     if (cudaMallocHost((void **)&s->hist_host, (size_t)kHistCap * 16) != cudaSuccess) return bail(DNS2D_ERR_NOMEM);
-    std::vector<float2> tw = twiddles(s->L);
-    if (cudaMemcpy(s->tw, tw.data(), L * 8, cudaMemcpyHostToDevice) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    std::vector<float2> tw = twiddles(*ks->cat);
+    if (cudaMemcpy(s->tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
     if (cudaMemset(s->counter, 0, 4) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
     if (cudaMemset(s->om2, 0, nom * 8) != cudaSuccess || cudaMemset(s->fnm1, 0, nom * 8) != cudaSuccess ||
         cudaMemset(s->work, 0, 2 * L * H * 8) != cudaSuccess || cudaMemset(s->phys, 0, 3 * L * L * 4) != cudaSuccess)
@@ -1428,13 +1446,19 @@ unsigned char *noalloc_scratch_address(int *err)
     return addr[dev];
 }
 
-// W_L^j built in FP64 and rounded once, on the device
-__global__ void k_noalloc_twiddles(float2 *tw, int L)
+// the per-stage twiddle tables of a catalog, built in FP64 on the device and rounded once
+__global__ void k_noalloc_twiddles(float2 *tw, TwCatalog c)
 {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < L; j += gridDim.x * blockDim.x) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < c.total; e += gridDim.x * blockDim.x) {
+        int i = 0;
+        while (i + 1 < c.n && c.off[i + 1] <= e) ++i;
+        const int R = c.R[i], NS = c.NS[i], M = R * NS;
+        const int loc = e - c.off[i];
+        const int r = loc / NS + 1, k = loc % NS;
+        const long long m = ((long long)r * k) % M;
         double sn, cs;
-        sincospi(2.0 * (double)j / (double)L, &sn, &cs);
-        tw[j] = make_float2((float)cs, (float)-sn);
+        sincospi(2.0 * (double)m / (double)M, &sn, &cs);
+        tw[e] = make_float2((float)cs, (float)-sn);
     }
 }
 
@@ -1457,7 +1481,7 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     const size_t o_om = o_work + align256(2 * L * H * sizeof(float2));
     const size_t o_fn = o_om + align256(nom * sizeof(float2));
     const size_t o_tw = o_fn + align256(nom * sizeof(float2));
-    const size_t o_prm = o_tw + align256(L * sizeof(float2));
+    const size_t o_prm = o_tw + align256((size_t)std::max(ks->cat->total, 1) * sizeof(float2));
     const size_t o_part = o_prm + align256(sizeof(StepParams));
     const size_t o_cnt = o_part + align256(H * sizeof(double2));
     const size_t o_hist = o_cnt + align256(sizeof(unsigned int));
@@ -1478,7 +1502,8 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     p.counter = reinterpret_cast<unsigned int *>(base + o_cnt);
     p.hist = reinterpret_cast<double2 *>(base + o_hist);
     // the array keeps the previous call's contents: rebuild twiddles, parameters and counter
-    k_noalloc_twiddles<<<(unsigned)((L + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(base + o_tw), (int)L);
+    k_noalloc_twiddles<<<(unsigned)((ks->cat->total + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(base + o_tw),
+                                                                                *ks->cat);
     k_set_params<<<1, 1, 0, st>>>(reinterpret_cast<StepParams *>(base + o_prm), dt, cnm1, cn, visc);
     k_noalloc_reset<<<1, 1, 0, st>>>(p.counter);
     dim3 tb(32, 8);

@@ -32,6 +32,10 @@ namespace dns2d {
 template <int N_>
 struct Cfg;
 
+// per-stage twiddle catalog of size N (defined below, after the large-grid plans)
+template <int N>
+struct TwCat;
+
 #define DNS2D_CFG(N_, ROWS_, NTB_, NTA_, ...)                                                  \
     template <>                                                                                \
     struct Cfg<N_> {                                                                           \
@@ -77,7 +81,7 @@ struct Pointers {
     float2 *om2;
     float2 *fnm1;
     float2 *work;
-    const float2 *tw;       // W_L^j, j in [0, L)
+    const float2 *tw;       // per-stage twiddle tables of the size's catalog (TwCat<N>)
     const StepParams *prm;
     double2 *part;          // per-column (E, Z) partial sums, [H]
     unsigned int *counter;  // arrival counter for the last-block reduction
@@ -172,7 +176,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p)
     const int z0 = blockIdx.x * ROWS;
     rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
     __syncthreads();
-    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
     // products: (u + i w)^2 = (u^2 - w^2) + i (2 u w)
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p)
         *a = make_float2(z.x * z.x - z.y * z.y, 2.0f * z.x * z.y);
     }
     __syncthreads();
-    fft_run<L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
     // unpack: D = F[u^2 - w^2] = (Q[k] + conj Q[L-k]) / 2, E = F[u w] = -i (Q[k] - conj Q[L-k]) / 4
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
@@ -234,7 +238,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p, int first
         sE[sidx(z)] = p.work[widx<L, H>(1, z, kx)];
     }
     __syncthreads();
-    fft_run<L, LP, false, 2, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, 2, NT>(smem, p.tw, typename C::Plan{});
 
     const StepParams prm = *p.prm;
     const float dt = prm.dt;
@@ -308,10 +312,241 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p, int first
         }
     }
     __syncthreads();
-    fft_run<L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
     for (int z = threadIdx.x; z < L; z += NT) {
         p.work[widx<L, H>(0, z, kx)] = sD[sidx(z)];
         p.work[widx<L, H>(1, z, kx)] = sE[sidx(z)];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Large-grid variants: one row / one column per CTA, one butterfly per thread and stage, three
+// stages.  Row pass: inverse plan (R1, R2, R3), forward plan (R3, R2, R1) so that the inverse's
+// last stage leaves in registers exactly the stride-L/R3 elements the forward's first stage
+// needs: C2R -> products -> R2C runs through shared memory only four times.  The first inverse
+// stage reads U, W straight from global memory.  Column pass: plan (R3, R2, R1) both ways, the
+// forward's first stage read from global, the inverse's last stage written to global.
+// ------------------------------------------------------------------------------------------
+template <int N_>
+struct Cfg2 {
+    static constexpr bool enabled = false;
+};
+
+#define DNS2D_CFG2(N_, NT_, R1_, R2_, R3_)                                                     \
+    template <>                                                                                \
+    struct Cfg2<N_> {                                                                          \
+        static constexpr bool enabled = true;                                                  \
+        static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, LP = SmemLen<L>::value;       \
+        static constexpr int NT = NT_, R1 = R1_, R2 = R2_, R3 = R3_;                           \
+        static_assert(R1_ * R2_ * R3_ == L, "plan");                                           \
+        static_assert(L / R1_ <= NT_ && L / R2_ <= NT_ && L / R3_ <= NT_, "one butterfly");    \
+    };
+DNS2D_CFG2(1024, 192, 16, 8, 12)
+DNS2D_CFG2(2048, 256, 16, 16, 12)
+DNS2D_CFG2(4096, 384, 16, 16, 24)
+#undef DNS2D_CFG2
+
+// twiddle catalog of size N: the stages of every plan compiled for it
+template <int N>
+constexpr TwCatalog make_catalog()
+{
+    TwCatalog c;
+    c.add(typename Cfg<N>::Plan{});
+    if constexpr (Cfg2<N>::enabled) {
+        c.add(Radices<Cfg2<N>::R1, Cfg2<N>::R2, Cfg2<N>::R3>{});
+        c.add(Radices<Cfg2<N>::R3, Cfg2<N>::R2, Cfg2<N>::R1>{});
+    }
+    return c;
+}
+
+template <int N>
+struct TwCat {
+    static constexpr TwCatalog cat = make_catalog<N>();
+    static constexpr int off(int R, int NS) { return cat.find(R, NS); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p)
+{
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3;
+    constexpr int LR1 = L / R1, LR3 = L / R3;
+    extern __shared__ float2 s[];
+    const int z = blockIdx.x;
+    const int j = threadIdx.x;
+    const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
+    const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
+    // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW
+    if (j < LR1) {
+        float2 v[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = j + r * LR1;
+            float2 a = make_float2(0.f, 0.f), b = a;
+            const bool lo = k < H, hi = k > L - H;
+            if (lo || hi) {
+                const int kk = lo ? k : L - k;
+                a = U[(size_t)kk << 2];
+                b = W[(size_t)kk << 2];
+            }
+            if (k == 0) v[r] = make_float2(a.x, b.x);
+            else if (lo) v[r] = make_float2(a.x - b.y, a.y + b.x);
+            else if (hi) v[r] = make_float2(a.x + b.y, b.x - a.y);
+            else v[r] = make_float2(0.f, 0.f);
+        }
+        DFT<R1, true>::run(v);
+        sm_store<L, R1, 1>(s, v, j);
+    }
+    stage1<TwCat<N>, L, R2, R1, true>(s, p.tw);
+    // inverse stage 3 into registers -> products -> forward stage 1
+    float2 v[R3];
+    __syncthreads();
+    if (j < LR3) {
+        sm_load<L, R3>(v, s, j);
+        bfly<TwCat<N>, L, R3, LR3, true>(v, j, p.tw);
+#pragma unroll
+        for (int q = 0; q < R3; ++q) v[q] = make_float2(v[q].x * v[q].x - v[q].y * v[q].y, 2.0f * v[q].x * v[q].y);
+        DFT<R3, false>::run(v);
+    }
+    __syncthreads();
+    if (j < LR3) sm_store<L, R3, 1>(s, v, j);
+    stage1<TwCat<N>, L, R2, R3, false>(s, p.tw);
+    stage1<TwCat<N>, L, R1, R3 * R2, false>(s, p.tw);
+    __syncthreads();
+    float2 *__restrict__ Do = p.work + widx<L, H>(0, z, 0);
+    float2 *__restrict__ Eo = p.work + widx<L, H>(1, z, 0);
+    for (int k = j; k < H; k += C::NT) {
+        const float2 q = s[sidx(k)];
+        const float2 m = s[sidx(k == 0 ? 0 : L - k)];
+        Do[(size_t)k << 2] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
+        Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p, int first, int hist_slot)
+{
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
+    constexpr int LR1 = L / R1, LR3 = L / R3;
+    extern __shared__ float2 smem[];
+    __shared__ double2 red[32];
+    __shared__ bool am_last;
+    const int kx = blockIdx.x;
+    const int j = threadIdx.x;
+    float2 *sD = smem, *sE = smem + LP;
+    float2 *om2c = p.om2 + (size_t)kx * N;
+    float2 *fnc = p.fnm1 + (size_t)kx * N;
+    // the state column is only needed after the forward transforms: start bringing it to L2
+    for (int o = j * 32; o < N; o += NT * 32) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(om2c + o));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(fnc + o));
+    }
+    // forward transforms of D and E along z, plan (R3, R2, R1): the twiddle-free radix-R3 first
+    // stage reads straight from global memory
+#pragma unroll 1
+    for (int a = 0; a < 2; ++a) {
+        float2 *s = a ? sE : sD;
+        if (j < LR3) {
+            // element j + r L/R3 of the column; L/R3 is a multiple of 4, so consecutive r are a
+            // fixed stride apart (one live address instead of R3)
+            static_assert(LR3 % 4 == 0, "stride");
+            constexpr size_t RS = (size_t)(LR3 / 4) * H * 4;
+            const float2 *ptr = p.work + widx<L, H>(a, j, kx);
+            float2 v[R3];
+#pragma unroll
+            for (int r = 0; r < R3; ++r, ptr += RS) v[r] = *ptr;
+            DFT<R3, false>::run(v);
+            sm_store<L, R3, 1>(s, v, j);
+        }
+        stage1<TwCat<N>, L, R2, R3, false>(s, p.tw);
+        stage1<TwCat<N>, L, R1, R3 * R2, false>(s, p.tw);
+    }
+    __syncthreads();
+
+    const StepParams prm = *p.prm;
+    const float dt = prm.dt;
+    const float cnm1 = first ? prm.cnm1_first : prm.cn;
+    const double hvdt = 0.5 * (double)prm.visc * (double)dt;
+    const double c2n = 0.5 * (double)dt * (2.0 + (double)cnm1);
+    const double c3n = -0.5 * (double)dt * (double)cnm1;
+    const float divxz = (float)(1.0 / ((double)L * (double)L));
+    double2 ez = make_double2(0.0, 0.0);
+    const double wgt = (kx == 0) ? 0.5 : 1.0;
+    for (int iz = j; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        const float2 d = sD[sidx(kzi)];
+        const float2 e = sE[sidx(kzi)];
+        float2 fn = make_float2(0.f, 0.f);
+        if (kz != -H) {
+            const float ga = (float)kz * (float)kx;
+            const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
+            fn.x = (ga * d.x + g2a2 * e.x) * divxz;
+            fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+        }
+        const double K2 = (double)kx * kx + (double)kz * kz;
+        const double arg = hvdt * K2;
+        const double inv = 1.0 / (1.0 + arg);
+        const float c1 = (float)((1.0 - arg) * inv);
+        const float c2 = (float)(c2n * inv);
+        const float c3 = (float)(c3n * inv);
+        const float2 om = om2c[iz];
+        const float2 fo = fnc[iz];
+        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        om2c[iz] = on;
+        fnc[iz] = fn;
+        float2 u, w;
+        double invK2;
+        recover_velocity(kx, kz, on, u, w, invK2);
+        sD[sidx(kzi)] = u;
+        sE[sidx(kzi)] = w;
+        const double pw = (double)on.x * on.x + (double)on.y * on.y;
+        ez.x += wgt * pw * invK2;
+        ez.y += wgt * pw;
+    }
+    for (int z = H + j; z < L - H; z += NT) {
+        sD[sidx(z)] = make_float2(0.f, 0.f);
+        sE[sidx(z)] = make_float2(0.f, 0.f);
+    }
+    ez = block_sum2<NT>(ez, red);
+    if (threadIdx.x == 0) {
+        p.part[kx] = ez;
+        __threadfence();
+        const unsigned int n = atomicAdd(p.counter, 1u);
+        am_last = (n == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (am_last) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int i = threadIdx.x; i < H; i += NT) {
+            const double2 q = __ldcg(&p.part[i]);
+            acc.x += q.x;
+            acc.y += q.y;
+        }
+        acc = block_sum2<NT>(acc, red);
+        if (threadIdx.x == 0) {
+            p.hist[hist_slot] = acc;
+            *p.counter = 0u;
+        }
+    }
+    // inverse transforms along z, plan (R3, R2, R1), the last stage straight to global memory
+#pragma unroll 1
+    for (int a = 0; a < 2; ++a) {
+        float2 *s = a ? sE : sD;
+        stage1<TwCat<N>, L, R3, 1, true>(s, p.tw);
+        stage1<TwCat<N>, L, R2, R3, true>(s, p.tw);
+        __syncthreads();
+        if (j < LR1) {
+            float2 v[R1];
+            sm_load<L, R1>(v, s, j);
+            bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
+            static_assert(LR1 % 4 == 0, "stride");
+            constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
+            float2 *ptr = p.work + widx<L, H>(a, j, kx);
+#pragma unroll
+            for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
+        }
     }
 }
 
@@ -354,7 +589,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p, const flo
         sW[sidx(z)] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_run<L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
     for (int z = threadIdx.x; z < L; z += NT) {
         p.work[widx<L, H>(0, z, kx)] = sU[sidx(z)];
         p.work[widx<L, H>(1, z, kx)] = sW[sidx(z)];
@@ -376,7 +611,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p, float
     const int z0 = blockIdx.x * ROWS;
     rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
     __syncthreads();
-    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
     float m = 0.0f;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
@@ -410,7 +645,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_from_phys(Pointers p, cons
         smem[r * LP + sidx(x)] = make_float2(phys[o], phys[(size_t)L * L + o]);
     }
     __syncthreads();
-    fft_run<L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
     const float sc = 1.0f / (float)L;
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
@@ -447,7 +682,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_scalar(Pointers p, float2 
     }
     for (int z = H + threadIdx.x; z < L - H; z += NT) smem[sidx(z)] = make_float2(0.f, 0.f);
     __syncthreads();
-    fft_run<L, LP, true, 1, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, 1, NT>(smem, p.tw, typename C::Plan{});
     for (int z = threadIdx.x; z < L; z += NT) scratch[widx<L, H>(0, z, kx)] = smem[sidx(z)];
 }
 
@@ -478,7 +713,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_scalar(Pointers p, const f
         smem[r * LP + sidx(k)] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_run<L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
     float mn = 3.402823466e38f, mx = -3.402823466e38f;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;

@@ -2,8 +2,8 @@
 //
 // A transform of compile-time length L runs as a sequence of radix-R stages
 // (radix plan = template list).  Each stage reads its R inputs per butterfly from shared
-// memory into registers, applies the inter-stage twiddles W_{Ns*R}^{r*k} (looked up in an
-// FP64-built, once-rounded table of W_L^j held in global memory / L1), performs the R-point
+// memory into registers, applies the inter-stage twiddles W_{Ns*R}^{r*k} (looked up in
+// FP64-built, once-rounded per-stage tables held in global memory / L1), performs the R-point
 // DFT fully unrolled in registers (generic Cooley-Tukey codelets whose constants are folded at
 // compile time) and writes the R outputs back in Stockham auto-sort order.  Several arrays
 // (rows or columns of the DNS fields) can be transformed together by one CTA.
@@ -268,14 +268,55 @@ constexpr int radix_product(Radices<Rs...>)
     return (1 * ... * Rs);
 }
 
+// ------------------------------------------------------------------------------------------
+// Per-stage twiddle tables.  Stage (R, Ns) of a length-L transform multiplies input r of
+// butterfly j by W_{Ns R}^{r k}, k = j mod Ns.  Its table holds those factors as [r-1][k]
+// (FP64-built, rounded once), so for fixed r the threads of a warp read consecutive entries.
+// A catalog lists the (R, Ns > 1) stages of every plan compiled for one L and their offsets in
+// one contiguous table; kernels get the table base and find their stage's offset at compile
+// time.
+// ------------------------------------------------------------------------------------------
+struct TwCatalog {
+    int n = 0;
+    int total = 0;
+    int R[64] = {};
+    int NS[64] = {};
+    int off[64] = {};
+    constexpr int find(int r, int ns) const
+    {
+        for (int i = 0; i < n; ++i)
+            if (R[i] == r && NS[i] == ns) return off[i];
+        return -1;
+    }
+    constexpr void add_plan(const int *rs, int nr)
+    {
+        int ns = 1;
+        for (int i = 0; i < nr; ++i) {
+            if (ns > 1 && find(rs[i], ns) < 0) {
+                R[n] = rs[i];
+                NS[n] = ns;
+                off[n] = total;
+                total += (rs[i] - 1) * ns;
+                ++n;
+            }
+            ns *= rs[i];
+        }
+    }
+    template <int... Rs>
+    constexpr void add(Radices<Rs...>)
+    {
+        const int a[] = {Rs...};
+        add_plan(a, (int)sizeof...(Rs));
+    }
+};
+
 // One Stockham stage over B arrays of length L (array b at s + b*LP).
-template <int L, int LP, int R, int NS, bool INV, int B, int NT>
+template <class Cat, int L, int LP, int R, int NS, bool INV, int B, int NT>
 __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *__restrict__ tw)
 {
     constexpr int LR = L / R;
     constexpr int TOT = B * LR;
     constexpr int NBF = (TOT + NT - 1) / NT;
-    constexpr int TSTEP = L / (NS * R);
     float2 v[NBF][R];
 #pragma unroll
     for (int i = 0; i < NBF; ++i) {
@@ -287,10 +328,12 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *
 #pragma unroll
             for (int r = 0; r < R; ++r) v[i][r] = x[sidx(j + r * LR)];
             if constexpr (NS > 1) {
-                const int k = j % NS;
+                constexpr int OFF = Cat::off(R, NS);
+                static_assert(OFF >= 0, "stage missing from the twiddle catalog");
+                const float2 *t = tw + OFF + j % NS;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    float2 w = __ldg(&tw[r * k * TSTEP]);
+                    float2 w = __ldg(t + (r - 1) * NS);
                     if constexpr (INV) w.y = -w.y;
                     v[i][r] = cmul(v[i][r], w);
                 }
@@ -315,18 +358,75 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *
     __syncthreads();
 }
 
-template <int L, int LP, bool INV, int B, int NT, int NS, int R0, int... Rs>
-__device__ __forceinline__ void fft_stages(float2 *s, const float2 *tw)
+// ------------------------------------------------------------------------------------------
+// One-butterfly-per-thread building blocks (the large-grid kernels).  Butterfly j of a stage
+// (radix R, Ns) reads x[j + r L/R] and writes y[(j/Ns) Ns R + j%Ns + q Ns]; with Ns = 1 the
+// reads of the first stage can come straight from global memory, and the last stage's outputs
+// (Ns = L/R: positions j + q L/R) can go straight back, skipping two shared-memory passes.
+// ------------------------------------------------------------------------------------------
+template <class Cat, int L, int R, int NS, bool INV>
+__device__ __forceinline__ void bfly(float2 (&v)[R], int j, const float2 *__restrict__ tw)
 {
-    fft_stage<L, LP, R0, NS, INV, B, NT>(s, tw);
-    if constexpr (sizeof...(Rs) > 0) fft_stages<L, LP, INV, B, NT, NS * R0, Rs...>(s, tw);
+    if constexpr (NS > 1) {
+        constexpr int OFF = Cat::off(R, NS);
+        static_assert(OFF >= 0, "stage missing from the twiddle catalog");
+        const float2 *t = tw + OFF + j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            float2 w = __ldg(t + (r - 1) * NS);
+            if constexpr (INV) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+    }
+    DFT<R, INV>::run(v);
 }
 
-template <int L, int LP, bool INV, int B, int NT, int... Rs>
+template <int L, int R>
+__device__ __forceinline__ void sm_load(float2 (&v)[R], const float2 *__restrict__ x, int j)
+{
+    constexpr int LR = L / R;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = x[sidx(j + r * LR)];
+}
+
+template <int L, int R, int NS>
+__device__ __forceinline__ void sm_store(float2 *__restrict__ y, const float2 (&v)[R], int j)
+{
+    const int k = j % NS;
+    const int base = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) y[sidx(base + q * NS)] = v[q];
+}
+
+// smem -> smem stage, one butterfly per thread (threads >= L/R idle); in place, so reads and
+// writes are separated by a barrier.  Leading barrier included; no trailing barrier.
+template <class Cat, int L, int R, int NS, bool INV>
+__device__ __forceinline__ void stage1(float2 *s, const float2 *tw)
+{
+    constexpr int LR = L / R;
+    const int j = threadIdx.x;
+    float2 v[R];
+    __syncthreads();
+    if (j < LR) {
+        sm_load<L, R>(v, s, j);
+        bfly<Cat, L, R, NS, INV>(v, j, tw);
+    }
+    __syncthreads();
+    if (j < LR) sm_store<L, R, NS>(s, v, j);
+}
+
+template <class Cat, int L, int LP, bool INV, int B, int NT, int NS, int R0, int... Rs>
+__device__ __forceinline__ void fft_stages(float2 *s, const float2 *tw)
+{
+    fft_stage<Cat, L, LP, R0, NS, INV, B, NT>(s, tw);
+    if constexpr (sizeof...(Rs) > 0) fft_stages<Cat, L, LP, INV, B, NT, NS * R0, Rs...>(s, tw);
+}
+
+template <class Cat, int L, int LP, bool INV, int B, int NT, int... Rs>
 __device__ __forceinline__ void fft_run(float2 *s, const float2 *tw, Radices<Rs...>)
 {
     static_assert((1 * ... * Rs) == L, "radix plan does not multiply to L");
-    fft_stages<L, LP, INV, B, NT, 1, Rs...>(s, tw);
+    fft_stages<Cat, L, LP, INV, B, NT, 1, Rs...>(s, tw);
 }
 
 }  // namespace dns2d

@@ -46,7 +46,7 @@ def test_initial_velocity_matches_oracle(N):
     assert s.scalars()["dt"] == pytest.approx(o.scalars()["dt"], rel=1e-6)
 
 
-@pytest.mark.parametrize("N", [16, 32, 64, 128, 256, 512, 1024, 2048])
+@pytest.mark.parametrize("N", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
 def test_twenty_steps_match_oracle(N):
     """20 steps, NEXTDT only at init, it = 1 and it = 20 (UPDATE > STEPS)."""
     steps, update = 20, 1000
