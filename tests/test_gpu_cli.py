@@ -1,0 +1,210 @@
+"""GPU tests of the drop-in mem_cuda CLI: stdout lines, signals, output files, restart.bin
+round trips, and restart.bin interchange with the reference's own binary (oracle/_ref/mem_cuda,
+built from the reference sources) when that binary is present."""
+import os
+import re
+import signal
+import subprocess
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(REPO, "optimizec_b200", "mem_cuda")
+REF = os.path.join(REPO, "oracle", "_ref", "mem_cuda")
+ITER_RE = re.compile(r"ITERATION\s+(\d+) T=([-0-9.eE]+) DT=([-0-9.eE]+) CN=([-0-9.eE]+) CFLM=([-0-9.eE]+) "
+                     r"Re=\s*([-0-9.eE+]+) VISC=\s*([-0-9.eE+]+) PALIN=(\d+) SIG=(\d+)")
+
+
+def iterations(text):
+    return {int(m[1]): dict(T=float(m[2]), DT=float(m[3]), CN=float(m[4]), CFLM=float(m[5]), SIG=int(m[9]))
+            for m in ITER_RE.finditer(text)}
+
+
+def run_cli(args, cwd, env=None, timeout=300, exe=CLI):
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    return subprocess.run([exe, *map(str, args)], cwd=cwd, env=e, capture_output=True, text=True, timeout=timeout)
+
+
+def test_cli_trajectory_matches_oracle(tmp_path):
+    """PAO start, N=128: every printed diagnostic line against the FP64 oracle."""
+    N, Re, K0, steps, cfl, update = 128, 1e4, 10.0, 60, 0.25, 20
+    p = run_cli([N, int(Re), int(K0), steps, cfl, update, 0], tmp_path)
+    assert p.returncode == 0, p.stderr
+    assert "PAO seed" in p.stdout and "[OUTPUT] Normal completion" in p.stdout
+    got = iterations(p.stdout)
+    assert sorted(got) == [1, 20, 40, 60]
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_pao()
+    done = 0
+    for it in sorted(got):
+        _, _, d = o.run(it - done, update, steps)
+        done = it
+        g = got[it]
+        assert g["T"] == pytest.approx(d[1], rel=1e-6)
+        assert g["DT"] == pytest.approx(d[2], rel=1e-5, abs=2e-8)
+        assert g["CN"] == pytest.approx(d[3], abs=2e-7)
+        assert g["CFLM"] == pytest.approx(d[4], rel=1e-6)
+        assert abs(g["SIG"] - int(d[5])) <= 1
+
+
+def _start(args, cwd, env=None):
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    return subprocess.Popen([CLI, *map(str, args)], cwd=cwd, env=e, stdout=subprocess.PIPE,
+                            stderr=subprocess.PIPE, text=True)
+
+
+def _wait_for(proc, pattern, timeout=60):
+    t0 = time.time()
+    buf = ""
+    while time.time() - t0 < timeout:
+        line = proc.stdout.readline()
+        if not line:
+            break
+        buf += line
+        if re.search(pattern, buf):
+            return buf
+    raise AssertionError(f"pattern {pattern!r} not seen; got:\n{buf[-2000:]}")
+
+
+def test_signals_save_restart_and_exit(tmp_path):
+    N = 64
+    proc = _start([N, 10000, 4, 1000000, 0.1, 10, 0], tmp_path)
+    try:
+        _wait_for(proc, r"ITERATION\s+20 ")
+        proc.send_signal(signal.SIGUSR1)
+        _wait_for(proc, r"Wrote .*meta\.csv")
+        proc.send_signal(signal.SIGRTMIN)
+        _wait_for(proc, r"_restart/meta\.csv")
+        proc.send_signal(signal.SIGHUP)
+        out, err = proc.communicate(timeout=60)
+    finally:
+        if proc.poll() is None:
+            proc.kill()
+    assert proc.returncode == 128 + signal.SIGHUP
+    folders = sorted(d for d in os.listdir(tmp_path) if d.startswith("output_64_4_1E04_0.10_"))
+    assert len(folders) >= 3, folders
+    rfold = [d for d in folders if d.endswith("_restart")]
+    assert len(rfold) == 1
+    for d in folders:
+        files = set(os.listdir(tmp_path / d))
+        for f in ["u_velocity.pgm", "v_velocity.pgm", "kinetic.pgm", "omega.pgm", "stream.pgm",
+                  "energy_spectrum.csv", "metrics.csv", "meta.csv"]:
+            assert f in files, (d, f)
+    L = 3 * N // 2
+    rb = tmp_path / rfold[0] / "restart.bin"
+    assert rb.stat().st_size == 144 + 3 * L * L * 4 + 2 * N * (N // 2) * 8
+    pgm = (tmp_path / rfold[0] / "omega.pgm").read_bytes()
+    assert pgm.startswith(f"P5\n{L} {L}\n255\n".encode())
+    meta = (tmp_path / rfold[0] / "meta.csv").read_text().splitlines()
+    assert meta[0].startswith("timestamp,N,K0,Re,CFL,visc,T,IT,Update")
+    assert meta[1].endswith(",CUDA")
+    # RESTART mode resumes from the folder at the saved iteration
+    it0 = int(meta[1].split(",")[7])
+    p = run_cli(["RESTART", str(tmp_path / rfold[0])], tmp_path, env={"RESTART_STEPS": str(it0 + 10)})
+    assert p.returncode == 0, p.stderr + p.stdout
+    assert f"at iteration {it0}" in p.stdout
+    assert max(iterations(p.stdout)) == it0 + 10
+
+
+def test_sigint_exits_without_files(tmp_path):
+    proc = _start([64, 10000, 4, 1000000, 0.1, 10, 0], tmp_path)
+    try:
+        _wait_for(proc, r"ITERATION\s+10 ")
+        proc.send_signal(signal.SIGINT)
+        out, _ = proc.communicate(timeout=60)
+    finally:
+        if proc.poll() is None:
+            proc.kill()
+    assert proc.returncode == 128 + signal.SIGINT
+    assert "exiting without saving" in out
+    assert not [d for d in os.listdir(tmp_path) if d.startswith("output_")]
+
+
+def test_restart_file_continues_exactly(tmp_path):
+    """restart.bin written after k steps and reloaded gives the same continuation."""
+    import optimizec_b200 as P
+    N = 128
+    s = P.Solver(N, 1e4, 4.0, 0.1)
+    s.init_k4(3)
+    s.next_dt()
+    s.step(1)
+    s.next_dt()
+    s.step(9)
+    path = str(tmp_path / "restart.bin")
+    s.save_restart(path)
+    a = run_cli([N, 10000, 4, 30, 0.1, 10, 0, path], tmp_path)
+    assert a.returncode == 0, a.stderr
+    s.step(10)
+    s.next_dt()
+    s.step(10)
+    s.next_dt()
+    got = iterations(a.stdout)
+    sc = s.scalars()
+    assert got[30]["T"] == pytest.approx(sc["t"], rel=1e-7)
+    assert got[30]["CFLM"] == pytest.approx(sc["cflm"], rel=1e-6)
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built")
+def test_restart_interchange_with_reference(tmp_path):
+    """A restart.bin written by this library is read by the reference's own mem_cuda, and both
+    continue along the same trajectory (printed T, DT, CN, CFLM, SIG)."""
+    import optimizec_b200 as P
+    N, Re, K0, cfl, update = 256, 1e4, 4.0, 0.1, 10
+    s = P.Solver(N, Re, K0, cfl)
+    s.init_k4(11)
+    s.next_dt()
+    path = str(tmp_path / "restart.bin")
+    s.save_restart(path)
+    args = [N, int(Re), int(K0), 40, cfl, update, 0, path]
+    ref = run_cli(args, tmp_path, exe=REF)
+    ours = run_cli(args, tmp_path)
+    assert ref.returncode == 0, ref.stderr
+    assert ours.returncode == 0, ours.stderr
+    r, o = iterations(ref.stdout), iterations(ours.stdout)
+    assert sorted(r) == sorted(o) == [1, 10, 20, 30, 40]
+    for it in r:
+        assert o[it]["T"] == pytest.approx(r[it]["T"], rel=1e-7)
+        assert o[it]["DT"] == pytest.approx(r[it]["DT"], rel=2e-6, abs=2e-8)
+        assert o[it]["CN"] == pytest.approx(r[it]["CN"], abs=2e-7)
+        assert o[it]["CFLM"] == pytest.approx(r[it]["CFLM"], rel=2e-6)
+        assert abs(o[it]["SIG"] - r[it]["SIG"]) <= 1
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ref_harness")),
+                    reason="reference harness not built")
+@pytest.mark.parametrize("N", [256, 512])
+def test_twenty_steps_match_reference_cufft(N, tmp_path):
+    """The reference's own cuFFT path from the same seeded field: vorticity after 20 steps
+    (relative L2 <= 1e-5) and the energy / enstrophy histories (1e-6 relative)."""
+    import optimizec_b200 as P
+    K0, Re, cfl, steps = 4.0, 1e4, 0.1, 20
+    om0 = O.k4_spectrum(N, K0, 5)
+    f = tmp_path / "om2.bin"
+    om0.tofile(f)
+    h = subprocess.run([os.path.join(REPO, "oracle", "_ref", "ref_harness"), str(N), str(Re), str(K0), str(cfl),
+                        str(steps), "1000", str(f), str(tmp_path / "ref")], capture_output=True, text=True,
+                       timeout=300)
+    assert h.returncode == 0, h.stderr
+    E_ref = np.array([float(l.split()[2]) for l in h.stdout.splitlines() if l.startswith("STEP ")])
+    om_ref = np.fromfile(tmp_path / "ref.om2", dtype=np.complex64).reshape(N, N // 2).astype(np.complex128)
+    s = P.Solver(N, Re, K0, cfl)
+    s.init_vorticity(om0)
+    s.next_dt()
+    E1, _ = s.step(1, history=True)
+    s.next_dt()
+    E2, _ = s.step(steps - 1, history=True)
+    E = np.concatenate([E1, E2])
+    om = s.om2().astype(np.complex128)
+    err = float(np.linalg.norm(om - om_ref) / np.linalg.norm(om_ref))
+    assert err <= 1e-5, err
+    assert np.max(np.abs(E / E_ref - 1)) <= 1e-6
