@@ -62,6 +62,7 @@ struct Launch {
         if constexpr (V2) {
             if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_cols_step3<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
         }
         if ((e = cudaFuncSetAttribute(k_rows_step<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
@@ -79,7 +80,9 @@ struct Launch {
     }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s)
     {
-        if constexpr (V2) k_cols_step2<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        // cp.async-filled columns pay off once a column is long enough (measured on B200)
+        if constexpr (V2 && N >= 4096) k_cols_step3<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        else if constexpr (V2) k_cols_step2<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         else k_cols_step<N><<<C::H, C::NTA, smA, s>>>(p, first, slot);
     }
     static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s)

@@ -551,6 +551,130 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p, int f
 }
 
 // ------------------------------------------------------------------------------------------
+// Column pass with asynchronous column loads: both columns (D, E) are requested with cp.async
+// at entry (no registers held by loads in flight); D's transform starts when D has landed while
+// E is still arriving; the state column is prefetched to L2.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p, int first, int hist_slot)
+{
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
+    constexpr int LR1 = L / R1, LR3 = L / R3;
+    extern __shared__ float2 smem[];
+    __shared__ double2 red[32];
+    __shared__ bool am_last;
+    const int kx = blockIdx.x;
+    const int j = threadIdx.x;
+    float2 *sD = smem, *sE = smem + LP;
+    float2 *om2c = p.om2 + (size_t)kx * N;
+    float2 *fnc = p.fnm1 + (size_t)kx * N;
+    for (int z = j; z < L; z += NT) cp_async8(sD + sidx(z), p.work + widx<L, H>(0, z, kx));
+    cp_async_commit();
+    for (int z = j; z < L; z += NT) cp_async8(sE + sidx(z), p.work + widx<L, H>(1, z, kx));
+    cp_async_commit();
+    for (int o = j * 16; o < N; o += NT * 16) {
+        prefetch_l2(om2c + o);
+        prefetch_l2(fnc + o);
+    }
+    // forward transforms along z, plan (R3, R2, R1); D starts while E is still landing
+    cp_async_wait<1>();
+    stage1<TwCat<N>, L, R3, 1, false>(sD, p.tw);
+    stage1<TwCat<N>, L, R2, R3, false>(sD, p.tw);
+    stage1<TwCat<N>, L, R1, R3 * R2, false>(sD, p.tw);
+    cp_async_wait<0>();
+    stage1<TwCat<N>, L, R3, 1, false>(sE, p.tw);
+    stage1<TwCat<N>, L, R2, R3, false>(sE, p.tw);
+    stage1<TwCat<N>, L, R1, R3 * R2, false>(sE, p.tw);
+    __syncthreads();
+
+    const StepParams prm = *p.prm;
+    const float dt = prm.dt;
+    const float cnm1 = first ? prm.cnm1_first : prm.cn;
+    const double hvdt = 0.5 * (double)prm.visc * (double)dt;
+    const double c2n = 0.5 * (double)dt * (2.0 + (double)cnm1);
+    const double c3n = -0.5 * (double)dt * (double)cnm1;
+    const float divxz = (float)(1.0 / ((double)L * (double)L));
+    double2 ez = make_double2(0.0, 0.0);
+    const double wgt = (kx == 0) ? 0.5 : 1.0;
+    for (int iz = j; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        const float2 d = sD[sidx(kzi)];
+        const float2 e = sE[sidx(kzi)];
+        float2 fn = make_float2(0.f, 0.f);
+        if (kz != -H) {
+            const float ga = (float)kz * (float)kx;
+            const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
+            fn.x = (ga * d.x + g2a2 * e.x) * divxz;
+            fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+        }
+        const double K2 = (double)kx * kx + (double)kz * kz;
+        const double arg = hvdt * K2;
+        const double inv = 1.0 / (1.0 + arg);
+        const float c1 = (float)((1.0 - arg) * inv);
+        const float c2 = (float)(c2n * inv);
+        const float c3 = (float)(c3n * inv);
+        const float2 om = om2c[iz];
+        const float2 fo = fnc[iz];
+        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        om2c[iz] = on;
+        fnc[iz] = fn;
+        float2 u, w;
+        double invK2;
+        recover_velocity(kx, kz, on, u, w, invK2);
+        sD[sidx(kzi)] = u;
+        sE[sidx(kzi)] = w;
+        const double pw = (double)on.x * on.x + (double)on.y * on.y;
+        ez.x += wgt * pw * invK2;
+        ez.y += wgt * pw;
+    }
+    for (int z = H + j; z < L - H; z += NT) {
+        sD[sidx(z)] = make_float2(0.f, 0.f);
+        sE[sidx(z)] = make_float2(0.f, 0.f);
+    }
+    ez = block_sum2<NT>(ez, red);
+    if (threadIdx.x == 0) {
+        p.part[kx] = ez;
+        __threadfence();
+        const unsigned int n = atomicAdd(p.counter, 1u);
+        am_last = (n == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (am_last) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int i = threadIdx.x; i < H; i += NT) {
+            const double2 q = __ldcg(&p.part[i]);
+            acc.x += q.x;
+            acc.y += q.y;
+        }
+        acc = block_sum2<NT>(acc, red);
+        if (threadIdx.x == 0) {
+            p.hist[hist_slot] = acc;
+            *p.counter = 0u;
+        }
+    }
+    // inverse transforms along z, plan (R3, R2, R1), the last stage straight to global memory
+#pragma unroll 1
+    for (int a = 0; a < 2; ++a) {
+        float2 *s = a ? sE : sD;
+        stage1<TwCat<N>, L, R3, 1, true>(s, p.tw);
+        stage1<TwCat<N>, L, R2, R3, true>(s, p.tw);
+        __syncthreads();
+        if (j < LR1) {
+            float2 v[R1];
+            sm_load<L, R1>(v, s, j);
+            bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
+            static_assert(LR1 % 4 == 0, "stride");
+            constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
+            float2 *ptr = p.work + widx<L, H>(a, j, kx);
+#pragma unroll
+            for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Column set-up: velocity spectrum -> U, W columns.
 // mode 0: from the compact velocity spectrum uw[iz][ix][2] (PAO); om2 = i (kz u - kx w)
 //         (CALCOM, cuda/calcom_cuda.cu:117-131), fnm1 = 0.

@@ -415,6 +415,20 @@ __device__ __forceinline__ void stage1(float2 *s, const float2 *tw)
     if (j < LR) sm_store<L, R, NS>(s, v, j);
 }
 
+// asynchronous global -> shared copies (cp.async; 8-byte elements, L1-allocating)
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <class Cat, int L, int LP, bool INV, int B, int NT, int NS, int R0, int... Rs>
 __device__ __forceinline__ void fft_stages(float2 *s, const float2 *tw)
 {
