@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="FP64 oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["dns4096", "ensemble"], default="dns4096",
+                    help="ensemble: the 64-member batched configuration (32xN=128, 24xN=256, 8xN=512)")
     return ap.parse_args()
 
 
@@ -359,9 +361,62 @@ def main_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def main_ensemble(args):
+    """64 independent decaying runs (32 x N=128, 24 x N=256, 8 x N=512; Re log-uniform in
+    [1e3, 1e5], K0 in [2, 8], seeds 0..63, CFL 0.1) advanced together; NEXTDT every UPDATE steps."""
+    import torch
+    import optimizec_b200 as P
+    ms = P.ensemble_members()
+    K, W, up = args.steps, args.warmup, WORKLOAD["UPDATE"]
+    b = P.Batch(ms)
+    b.init_k4()
+    b.next_dt()
+    it = 0
+
+    def advance(to):
+        nonlocal it
+        while it < to:
+            nxt = 1 if it < 1 else min(to, (it // up + 1) * up)
+            b.step(nxt - it)
+            it = nxt
+            if it == 1 or it % up == 0:
+                b.next_dt()
+    advance(W)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream(), device=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    advance(W + K)
+    e1.record(stream)
+    b.sync()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms_ = e0.elapsed_time(e1)
+    member_steps = len(ms) * K / (ms_ / 1e3)
+    pts = sum(m[0] ** 2 for m in ms)
+    peak, peak_kind = measured_peaks()
+    byts = sum(64 * m[0] ** 2 for m in ms)
+    line = {"metric": "member-steps/s (64-member batched 2D DNS ensemble)", "value": round(member_steps, 1),
+            "unit": "member-steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": round(ms_ / K, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ensemble 32xN=128 + 24xN=256 + 8xN=512, Re log-uniform [1e3,1e5], "
+                                   "K0 in [2,8], seeds 0..63, CFL 0.1, UPDATE 100, one graph per chunk"},
+            "ensemble_steps_per_s": round(K / (ms_ / 1e3), 2),
+            "mpts_steps_per_s": round(pts * K / (ms_ / 1e3) / 1e6, 1),
+            "hbm_frac_64N2": round(byts * K / (ms_ / 1e3) / (peak * 1e9), 4), "clocks": ck}
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.workload == "ensemble" and a.impl == "ours":
+        main_ensemble(a)
+    elif a.impl == "reference":
         main_reference(a)
     else:
         main_ours(a)

@@ -135,6 +135,31 @@ int dns2d_load_restart(dns2d_state *s, const char *path);
 int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float cn, int nsteps,
                        void *om2, void *fnm1, void *stream);
 
+/* ---- batched ensembles (no counterpart in the reference: written for its ensemble
+ * configuration).  Independent runs, each with its own N (any supported size), Re, K0, CFL
+ * and initial-field seed, advanced together: members of one N share each kernel launch, and a
+ * chunk of up to 128 ensemble steps is one captured CUDA graph.  Every member keeps the
+ * reference's float scalar bookkeeping; results equal those of one dns2d_state per member. */
+typedef struct {
+    int32_t N;
+    float Re, K0, cflnum;
+    uint64_t seed; /* seed of the k^4 exp(-2 (k/K0)^2) initial field (dns2d_batch_init_k4) */
+} dns2d_member;
+typedef struct dns2d_batch dns2d_batch;
+int dns2d_batch_create(dns2d_batch **out, const dns2d_member *members, int count, int device);
+void dns2d_batch_destroy(dns2d_batch *b);
+const char *dns2d_batch_last_error(const dns2d_batch *b);
+void *dns2d_batch_stream(dns2d_batch *b);
+/* every member from its own seeded k^4 field (then call dns2d_batch_next_dt) */
+int dns2d_batch_init_k4(dns2d_batch *b);
+/* NEXTDT for every member; cflm (nullable) receives count values */
+int dns2d_batch_next_dt(dns2d_batch *b, float *cflm);
+/* nsteps steps of every member; E_hist / Z_hist (nullable) are [count][nsteps] */
+int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, double *Z_hist);
+int dns2d_batch_sync(dns2d_batch *b);
+int dns2d_batch_get_om2(dns2d_batch *b, int member, float *om2);
+int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars *out);
+
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);
 /* ms[0..3], counts[0..3]: row pass, column pass, NEXTDT/CFLM, OM2PHYS+sigma */

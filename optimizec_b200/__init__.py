@@ -36,6 +36,9 @@ SYMBOLS = [
     "dns2d_velocity_spectrum_bins", "dns2d_get_scalars", "dns2d_set_scalars", "dns2d_get_om2",
     "dns2d_get_fnm1", "dns2d_get_phys", "dns2d_set_velocity_phys", "dns2d_save_restart",
     "dns2d_load_restart", "dns2d_phase_timing", "dns2d_phase_report", "dns2d_step_noalloc",
+    "dns2d_batch_create", "dns2d_batch_destroy", "dns2d_batch_last_error", "dns2d_batch_stream",
+    "dns2d_batch_init_k4", "dns2d_batch_next_dt", "dns2d_batch_step", "dns2d_batch_sync",
+    "dns2d_batch_get_om2", "dns2d_batch_get_scalars",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -55,6 +58,11 @@ class Scalars(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Member(C.Structure):
+    _fields_ = [("N", C.c_int32), ("Re", C.c_float), ("K0", C.c_float), ("cflnum", C.c_float),
+                ("seed", C.c_uint64)]
 
 
 def build(verbose: bool = False) -> str:
@@ -123,6 +131,16 @@ def lib():
         "dns2d_phase_report": (C.c_int, [vp, dp, C.POINTER(C.c_longlong)]),
         "dns2d_step_noalloc": (C.c_int, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
                                          vp, vp, vp]),
+        "dns2d_batch_create": (C.c_int, [C.POINTER(vp), C.POINTER(Member), C.c_int, C.c_int]),
+        "dns2d_batch_destroy": (None, [vp]),
+        "dns2d_batch_last_error": (C.c_char_p, [vp]),
+        "dns2d_batch_stream": (vp, [vp]),
+        "dns2d_batch_init_k4": (C.c_int, [vp]),
+        "dns2d_batch_next_dt": (C.c_int, [vp, fp]),
+        "dns2d_batch_step": (C.c_int, [vp, C.c_int, dp, dp]),
+        "dns2d_batch_sync": (C.c_int, [vp]),
+        "dns2d_batch_get_om2": (C.c_int, [vp, C.c_int, fp]),
+        "dns2d_batch_get_scalars": (C.c_int, [vp, C.c_int, C.POINTER(Scalars)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -311,3 +329,89 @@ class Solver:
         n = np.zeros(4, dtype=np.int64)
         self._chk(self._L.dns2d_phase_report(self._s, _dp(ms), n.ctypes.data_as(C.POINTER(C.c_longlong))))
         return ms, n
+
+
+class Batch:
+    """An ensemble of independent runs advanced together (dns2d_batch_*)."""
+
+    def __init__(self, members, device: int = 0):
+        """members: sequence of (N, Re, K0, cfl, seed)"""
+        self._L = lib()
+        self.members = [tuple(m) for m in members]
+        arr = (Member * len(self.members))(*[Member(int(N), Re, K0, c, int(sd)) for N, Re, K0, c, sd in self.members])
+        self._b = C.c_void_p()
+        rc = self._L.dns2d_batch_create(C.byref(self._b), arr, len(self.members), device)
+        if rc:
+            raise Dns2dError(f"dns2d_batch_create: {self._L.dns2d_strerror(rc).decode()}")
+
+    def _chk(self, rc):
+        if rc:
+            raise Dns2dError(f"{self._L.dns2d_strerror(rc).decode()}: {self._L.dns2d_batch_last_error(self._b).decode()}")
+
+    def close(self):
+        if self._b:
+            self._L.dns2d_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_k4(self):
+        self._chk(self._L.dns2d_batch_init_k4(self._b))
+
+    def next_dt(self) -> np.ndarray:
+        out = np.zeros(len(self.members), dtype=np.float32)
+        self._chk(self._L.dns2d_batch_next_dt(self._b, _fp(out)))
+        return out
+
+    def step(self, n: int, history: bool = False):
+        if history:
+            E = np.zeros((len(self.members), n))
+            Z = np.zeros((len(self.members), n))
+            self._chk(self._L.dns2d_batch_step(self._b, n, _dp(E), _dp(Z)))
+            return E, Z
+        self._chk(self._L.dns2d_batch_step(self._b, n, None, None))
+        return None
+
+    def sync(self):
+        self._chk(self._L.dns2d_batch_sync(self._b))
+
+    def stream(self) -> int:
+        return self._L.dns2d_batch_stream(self._b) or 0
+
+    def om2(self, m: int) -> np.ndarray:
+        N = self.members[m][0]
+        out = np.zeros((N, N // 2), dtype=np.complex64)
+        self._chk(self._L.dns2d_batch_get_om2(self._b, m, _fp(out.view(np.float32))))
+        return out
+
+    def scalars(self, m: int) -> dict:
+        s = Scalars()
+        self._chk(self._L.dns2d_batch_get_scalars(self._b, m, C.byref(s)))
+        return s.as_dict()
+
+
+def ensemble_members(counts=((128, 32), (256, 24), (512, 8)), cfl: float = 0.1):
+    """The 64-member ensemble configuration: sizes by count, seeds 0..63, Re log-uniform in
+    [1e3, 1e5] and K0 uniform-integer in [2, 8], both drawn from splitmix64(seed)."""
+    def sm64(x):
+        x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        return x ^ (x >> 31)
+    out = []
+    seed = 0
+    for N, n in counts:
+        for _ in range(n):
+            r1 = sm64(seed)
+            r2 = sm64(r1)
+            u1 = (r1 >> 11) / float(1 << 53)
+            u2 = (r2 >> 11) / float(1 << 53)
+            Re = 10.0 ** (3.0 + 2.0 * u1)
+            K0 = float(2 + min(6, int(7 * u2)))
+            out.append((N, Re, K0, cfl, seed))
+            seed += 1
+    return out

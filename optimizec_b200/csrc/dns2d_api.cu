@@ -35,10 +35,10 @@ struct KernelSet {
     int rows_blocks;
     const TwCatalog *cat;
     cudaError_t (*setup)();
-    void (*rows_step)(const Pointers &, cudaStream_t);
-    void (*cols_step)(const Pointers &, int, int, cudaStream_t);
-    void (*cols_init)(const Pointers &, const float2 *, int, cudaStream_t);
-    void (*rows_velocity)(const Pointers &, float *, float *, float, cudaStream_t);
+    void (*rows_step)(const Pointers &, cudaStream_t, int);
+    void (*cols_step)(const Pointers &, int, int, cudaStream_t, int);
+    void (*cols_init)(const Pointers &, const float2 *, int, cudaStream_t, int);
+    void (*rows_velocity)(const Pointers &, float *, float *, float, cudaStream_t, int);
     void (*rows_from_phys)(const Pointers &, const float *, cudaStream_t);
     void (*cols_scalar)(const Pointers &, float2 *, int, cudaStream_t);
     void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
@@ -73,25 +73,25 @@ struct Launch {
         if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
         return cudaSuccess;
     }
-    static void rows_step(const Pointers &p, cudaStream_t s)
+    static void rows_step(const Pointers &p, cudaStream_t s, int ny)
     {
-        if constexpr (V2) k_rows_step2<N><<<C::L, Cfg2<N>::NT, sm2, s>>>(p);
-        else k_rows_step<N><<<GB, C::NTB, smB, s>>>(p);
+        if constexpr (V2) k_rows_step2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p);
+        else k_rows_step<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p);
     }
-    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s)
+    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
     {
         // cp.async-filled columns pay off once a column is long enough (measured on B200)
-        if constexpr (V2 && N >= 4096) k_cols_step3<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
-        else if constexpr (V2) k_cols_step2<N><<<C::H, Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
-        else k_cols_step<N><<<C::H, C::NTA, smA, s>>>(p, first, slot);
+        if constexpr (V2 && N >= 4096) k_cols_step3<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        else if constexpr (V2) k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        else k_cols_step<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
     }
-    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s)
+    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
     {
-        k_cols_init<N><<<C::H, C::NTA, smA, s>>>(p, uw, mode);
+        k_cols_init<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, uw, mode);
     }
-    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s)
+    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s, int ny)
     {
-        k_rows_velocity<N><<<GB, C::NTB, smB, s>>>(p, phys, cflm, dx);
+        k_rows_velocity<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p, phys, cflm, dx);
     }
     static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
     {
@@ -353,6 +353,10 @@ struct dns2d_state {
         p.part = part;
         p.counter = counter;
         p.hist = hist;
+        p.s_state = 0;
+        p.s_work = 0;
+        p.s_part = 0;
+        p.s_hist = 0;
         return p;
     }
 };
@@ -765,7 +769,7 @@ extern "C" int dns2d_init_pao(dns2d_state *s, double *stats19, int *pao_seed)
     if (bytes > 3 * (size_t)s->L * s->L * 4) return fail(s, DNS2D_ERR_NOMEM, "PAO staging");
     d_uw = reinterpret_cast<float2 *>(s->phys);
     DNS2D_CUDA(cudaMemcpyAsync(d_uw, uw.data(), bytes, cudaMemcpyHostToDevice, s->stream), "PAO upload");
-    s->ks->cols_init(s->ptrs(), d_uw, 0, s->stream);
+    s->ks->cols_init(s->ptrs(), d_uw, 0, s->stream, 1);
     DNS2D_LAUNCHED("cols_init(PAO)");
     DNS2D_CUDA(cudaStreamSynchronize(s->stream), "PAO init");
     s->initialised = true;
@@ -785,7 +789,7 @@ extern "C" int dns2d_init_vorticity(dns2d_state *s, const float *om2, const floa
     } else {
         DNS2D_CUDA(cudaMemsetAsync(s->fnm1, 0, (size_t)s->N * s->H * 8, s->stream), "fnm1 clear");
     }
-    s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream);
+    s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream, 1);
     DNS2D_LAUNCHED("cols_init(om2)");
     DNS2D_CUDA(cudaStreamSynchronize(s->stream), "vorticity init");
     s->initialised = true;
@@ -868,8 +872,8 @@ int get_graph(dns2d_state *s, int first, int K, cudaGraphExec_t *out)
     DNS2D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     const Pointers p = s->ptrs();
     for (int i = 0; i < K; ++i) {
-        s->ks->rows_step(p, s->stream);
-        s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream);
+        s->ks->rows_step(p, s->stream, 1);
+        s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream, 1);
     }
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     if (e != cudaSuccess) return cuda_check(s, e, "end capture");
@@ -901,11 +905,11 @@ extern "C" int dns2d_step(dns2d_state *s, int nsteps, double *E_hist, double *Z_
             const Pointers p = s->ptrs();
             for (int i = 0; i < K; ++i) {
                 phase_begin(s);
-                s->ks->rows_step(p, s->stream);
+                s->ks->rows_step(p, s->stream, 1);
                 DNS2D_LAUNCHED("rows_step");
                 phase_end(s, 0);
                 phase_begin(s);
-                s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream);
+                s->ks->cols_step(p, (first && i == 0) ? 1 : 0, i, s->stream, 1);
                 DNS2D_LAUNCHED("cols_step");
                 phase_end(s, 1);
             }
@@ -963,7 +967,7 @@ int compute_cflm(dns2d_state *s, float *out)
     const float PI = 3.14159265358979323846f;
     const float DX = 2.0f * PI / float(s->N);
     DNS2D_CUDA(cudaMemsetAsync(s->cflm_dev, 0, 4, s->stream), "cflm clear");
-    s->ks->rows_velocity(s->ptrs(), nullptr, s->cflm_dev, DX, s->stream);
+    s->ks->rows_velocity(s->ptrs(), nullptr, s->cflm_dev, DX, s->stream, 1);
     DNS2D_LAUNCHED("rows_velocity(cfl)");
     float h = 0.0f;
     DNS2D_CUDA(cudaMemcpyAsync(&h, s->cflm_dev, 4, cudaMemcpyDeviceToHost, s->stream), "cflm copy");
@@ -1031,7 +1035,7 @@ extern "C" int dns2d_velocity_phys(dns2d_state *s)
 {
     if (!s) return DNS2D_ERR_ARG;
     if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
-    s->ks->rows_velocity(s->ptrs(), s->phys, nullptr, 1.0f, s->stream);
+    s->ks->rows_velocity(s->ptrs(), s->phys, nullptr, 1.0f, s->stream, 1);
     DNS2D_LAUNCHED("rows_velocity(phys)");
     return DNS2D_OK;
 }
@@ -1368,7 +1372,7 @@ extern "C" int dns2d_load_restart(dns2d_state *s, const char *path)
     if (h.v1.version >= 2) {
         rc = dns2d_set_velocity_phys(s, u.data(), w.data());
     } else {
-        s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream);  // velocity from OM2 (v1)
+        s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream, 1);  // velocity from OM2 (v1)
         rc = cuda_check(s, cudaStreamSynchronize(s->stream), "v1 velocity");
     }
     if (rc) return rc;
@@ -1408,6 +1412,391 @@ extern "C" int dns2d_phase_report(dns2d_state *s, double *ms, long long *counts)
         if (ms) ms[i] = s->phase_ms[i];
         if (counts) counts[i] = s->phase_n[i];
     }
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// Batched ensembles: independent runs of (possibly different) N, Re, K0, CFL advanced together.
+// Members are grouped by N; each group's state, work buffer and parameter blocks are contiguous
+// and every kernel of a group covers all its members in one launch (member = blockIdx.y).  A
+// chunk of up to 128 ensemble steps (row + column pass of every group) is one captured CUDA
+// graph.  Each member keeps the reference's float scalar bookkeeping on the host.
+// ============================================================================================
+namespace {
+
+struct BatchGroup {
+    int N = 0, H = 0, L = 0, count = 0;
+    const KernelSet *ks = nullptr;
+    std::vector<int> members;  // batch indices of this group's members, in group order
+    float2 *om2 = nullptr, *fnm1 = nullptr, *work = nullptr, *tw = nullptr;
+    StepParams *prm = nullptr;
+    double2 *part = nullptr, *hist = nullptr;
+    unsigned int *counter = nullptr;
+    float *cflm = nullptr;
+
+    Pointers ptrs() const
+    {
+        Pointers p;
+        p.om2 = om2;
+        p.fnm1 = fnm1;
+        p.work = work;
+        p.tw = tw;
+        p.prm = prm;
+        p.part = part;
+        p.counter = counter;
+        p.hist = hist;
+        p.s_state = (size_t)N * H;
+        p.s_work = 2 * (size_t)L * H;
+        p.s_part = H;
+        p.s_hist = kChunk;
+        return p;
+    }
+};
+
+struct MemberScalars {
+    float Re, K0, visc, t, dt, cn, cnm1, cflnum, cflm;
+    int it, ifn;
+    uint64_t seed;
+};
+
+}  // namespace
+
+struct dns2d_batch {
+    int count = 0, device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<MemberScalars> sc;
+    std::vector<std::pair<int, int>> where;  // member -> (group, index in group)
+    std::vector<BatchGroup> groups;
+    StepParams *prm_host = nullptr;  // pinned, count entries (group order)
+    double2 *hist_host = nullptr;    // pinned, count * kChunk entries
+    float *cflm_host = nullptr;      // pinned, count entries
+    cudaEvent_t prm_copied = nullptr;
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    bool initialised = false;
+    std::string err;
+};
+
+namespace {
+
+int bfail(dns2d_batch *b, int code, const char *what, cudaError_t e = cudaSuccess)
+{
+    if (b) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "%s%s%s", what, e != cudaSuccess ? ": " : "",
+                      e != cudaSuccess ? cudaGetErrorString(e) : "");
+        b->err = buf;
+    }
+    return code;
+}
+
+#define BATCH_CUDA(call, what)                                                   \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) return bfail(b, DNS2D_ERR_CUDA, what, e_);        \
+    } while (0)
+
+}  // namespace
+
+extern "C" void dns2d_batch_destroy(dns2d_batch *b)
+{
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    for (BatchGroup &g : b->groups) {
+        cudaFree(g.om2);
+        cudaFree(g.fnm1);
+        cudaFree(g.work);
+        cudaFree(g.tw);
+        cudaFree(g.prm);
+        cudaFree(g.part);
+        cudaFree(g.hist);
+        cudaFree(g.counter);
+        cudaFree(g.cflm);
+    }
+    if (b->prm_host) cudaFreeHost(b->prm_host);
+    if (b->hist_host) cudaFreeHost(b->hist_host);
+    if (b->cflm_host) cudaFreeHost(b->cflm_host);
+    if (b->prm_copied) cudaEventDestroy(b->prm_copied);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+extern "C" const char *dns2d_batch_last_error(const dns2d_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+extern "C" void *dns2d_batch_stream(dns2d_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+extern "C" int dns2d_batch_create(dns2d_batch **out, const dns2d_member *members, int count, int device)
+{
+    if (!out || !members || count <= 0) return DNS2D_ERR_ARG;
+    *out = nullptr;
+    for (int i = 0; i < count; ++i)
+        if (!kernel_set(members[i].N)) return DNS2D_ERR_SIZE;
+    dns2d_batch *b = new dns2d_batch();
+    b->count = count;
+    b->device = device;
+    auto bail = [&](int rc) {
+        dns2d_batch_destroy(b);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&b->prm_copied, cudaEventDisableTiming) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    b->sc.resize((size_t)count);
+    b->where.resize((size_t)count);
+    for (int i = 0; i < count; ++i) {
+        const dns2d_member &m = members[i];
+        int gi = -1;
+        for (size_t k = 0; k < b->groups.size(); ++k)
+            if (b->groups[k].N == m.N) gi = (int)k;
+        if (gi < 0) {
+            BatchGroup g;
+            g.N = m.N;
+            g.H = m.N / 2;
+            g.L = 3 * m.N / 2;
+            g.ks = kernel_set(m.N);
+            b->groups.push_back(g);
+            gi = (int)b->groups.size() - 1;
+        }
+        BatchGroup &g = b->groups[(size_t)gi];
+        b->where[(size_t)i] = {gi, g.count};
+        g.members.push_back(i);
+        g.count += 1;
+        MemberScalars &c = b->sc[(size_t)i];
+        c = MemberScalars{m.Re, m.K0, float(1.0 / m.Re), 0.0f, 0.0f, 1.0f, 0.0f, m.cflnum, 0.0f, 0, 1, m.seed};
+    }
+    for (BatchGroup &g : b->groups) {
+        if (g.ks->setup() != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+        const size_t H = g.H, L = g.L, nom = (size_t)g.N * H, c = (size_t)g.count;
+        auto dalloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+        if (!dalloc((void **)&g.om2, c * nom * 8) || !dalloc((void **)&g.fnm1, c * nom * 8) ||
+            !dalloc((void **)&g.work, c * 2 * L * H * 8) ||
+            !dalloc((void **)&g.tw, (size_t)std::max(g.ks->cat->total, 1) * 8) ||
+            !dalloc((void **)&g.prm, c * sizeof(StepParams)) || !dalloc((void **)&g.part, c * H * 16) ||
+            !dalloc((void **)&g.hist, c * kChunk * 16) || !dalloc((void **)&g.counter, c * 4) ||
+            !dalloc((void **)&g.cflm, c * 4)) {
+            cudaGetLastError();
+            return bail(DNS2D_ERR_NOMEM);
+        }
+        std::vector<float2> tw = twiddles(*g.ks->cat);
+        if (cudaMemcpy(g.tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(g.counter, 0, c * 4) != cudaSuccess || cudaMemset(g.fnm1, 0, c * nom * 8) != cudaSuccess)
+            return bail(DNS2D_ERR_CUDA);
+    }
+    if (cudaMallocHost((void **)&b->prm_host, (size_t)count * sizeof(StepParams)) != cudaSuccess ||
+        cudaMallocHost((void **)&b->hist_host, (size_t)count * kChunk * 16) != cudaSuccess ||
+        cudaMallocHost((void **)&b->cflm_host, (size_t)count * 4) != cudaSuccess)
+        return bail(DNS2D_ERR_NOMEM);
+    *out = b;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_init_vorticity(dns2d_batch *b, int member, const float *om2)
+{
+    if (!b || !om2 || member < 0 || member >= b->count) return DNS2D_ERR_ARG;
+    const auto [gi, k] = b->where[(size_t)member];
+    BatchGroup &g = b->groups[(size_t)gi];
+    const size_t nom = (size_t)g.N * g.H;
+    float2 *stage = g.work + (size_t)k * 2 * g.L * g.H;  // the member's work buffer as staging
+    BATCH_CUDA(cudaMemcpyAsync(stage, om2, nom * 8, cudaMemcpyHostToDevice, b->stream), "om2 upload");
+    dim3 tb(32, 8), tg((g.H + 31) / 32, (g.N + 31) / 32);
+    k_transpose_c64<<<tg, tb, 0, b->stream>>>(stage, g.om2 + (size_t)k * nom, g.N, g.H);
+    BATCH_CUDA(cudaGetLastError(), "transpose");
+    BATCH_CUDA(cudaMemsetAsync(g.fnm1 + (size_t)k * nom, 0, nom * 8, b->stream), "fnm1 clear");
+    MemberScalars &c = b->sc[(size_t)member];
+    c.it = 0;
+    c.t = 0.0f;
+    c.dt = 0.0f;
+    c.cn = 1.0f;
+    c.cnm1 = 0.0f;
+    c.visc = float(1.0 / c.Re);
+    BATCH_CUDA(cudaStreamSynchronize(b->stream), "vorticity upload");
+    return DNS2D_OK;
+}
+
+// velocity of every member from its vorticity (after the vorticity uploads)
+static int batch_velocity(dns2d_batch *b)
+{
+    for (BatchGroup &g : b->groups) g.ks->cols_init(g.ptrs(), nullptr, 1, b->stream, g.count);
+    BATCH_CUDA(cudaGetLastError(), "cols_init(batch)");
+    BATCH_CUDA(cudaStreamSynchronize(b->stream), "batch velocity");
+    b->initialised = true;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_init_k4(dns2d_batch *b)
+{
+    if (!b) return DNS2D_ERR_ARG;
+    for (int i = 0; i < b->count; ++i) {
+        const auto [gi, k] = b->where[(size_t)i];
+        const int N = b->groups[(size_t)gi].N;
+        std::vector<float> om((size_t)N * (N / 2) * 2);
+        dns2d_k4_spectrum(N, b->sc[(size_t)i].K0, b->sc[(size_t)i].seed, om.data());
+        int rc = dns2d_batch_init_vorticity(b, i, om.data());
+        if (rc) return rc;
+    }
+    return batch_velocity(b);
+}
+
+extern "C" int dns2d_batch_next_dt(dns2d_batch *b, float *cflm_out)
+{
+    if (!b) return DNS2D_ERR_ARG;
+    if (!b->initialised) return bfail(b, DNS2D_ERR_STATE, "no initial condition");
+    for (BatchGroup &g : b->groups) {
+        BATCH_CUDA(cudaMemsetAsync(g.cflm, 0, (size_t)g.count * 4, b->stream), "cflm clear");
+        const float DX = 2.0f * 3.14159265358979323846f / float(g.N);
+        g.ks->rows_velocity(g.ptrs(), nullptr, g.cflm, DX, b->stream, g.count);
+        BATCH_CUDA(cudaGetLastError(), "rows_velocity(batch)");
+    }
+    int off = 0;
+    for (BatchGroup &g : b->groups) {
+        BATCH_CUDA(cudaMemcpyAsync(b->cflm_host + off, g.cflm, (size_t)g.count * 4, cudaMemcpyDeviceToHost, b->stream),
+                   "cflm copy");
+        off += g.count;
+    }
+    BATCH_CUDA(cudaStreamSynchronize(b->stream), "cflm sync");
+    const float PI = 3.14159265358979323846f;
+    off = 0;
+    for (BatchGroup &g : b->groups) {
+        for (int k = 0; k < g.count; ++k) {
+            MemberScalars &c = b->sc[(size_t)g.members[(size_t)k]];
+            const float CFLM = b->cflm_host[off + k];
+            if (c.it == 0 && c.dt == 0.0f) {  // NEXTDT init branch (cuda/dns_cuda.cu:562-569)
+                c.dt = c.cflnum / CFLM / PI;
+                c.cflm = CFLM;
+            } else if (c.ifn > 0 && (c.it % c.ifn) == 0) {  // regular update (:572-579)
+                const float CFL = CFLM * c.dt * PI;
+                c.cn = 0.8f + 0.2f * (c.cflnum / CFL);
+                c.dt = c.dt * c.cn;
+                c.cflm = CFLM;
+            }
+            if (cflm_out) cflm_out[g.members[(size_t)k]] = c.cflm;
+        }
+        off += g.count;
+    }
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, double *Z_hist)
+{
+    if (!b || nsteps < 0) return DNS2D_ERR_ARG;
+    if (!b->initialised) return bfail(b, DNS2D_ERR_STATE, "no initial condition");
+    // parameter blocks of every member (group order), copied once per call
+    BATCH_CUDA(cudaEventSynchronize(b->prm_copied), "parameter buffer");
+    int off = 0;
+    for (BatchGroup &g : b->groups) {
+        for (int k = 0; k < g.count; ++k) {
+            const MemberScalars &c = b->sc[(size_t)g.members[(size_t)k]];
+            b->prm_host[off + k] = StepParams{c.dt, c.cnm1, c.cn, c.visc};
+        }
+        BATCH_CUDA(cudaMemcpyAsync(g.prm, b->prm_host + off, (size_t)g.count * sizeof(StepParams),
+                                   cudaMemcpyHostToDevice, b->stream),
+                   "parameter copy");
+        off += g.count;
+    }
+    BATCH_CUDA(cudaEventRecord(b->prm_copied, b->stream), "parameter event");
+    int done = 0;
+    while (done < nsteps) {
+        const int K = std::min(kChunk, nsteps - done);
+        const int first = (done == 0) ? 1 : 0;
+        auto key = std::make_pair(first, K);
+        auto itg = b->graphs.find(key);
+        cudaGraphExec_t ex = nullptr;
+        if (itg != b->graphs.end()) {
+            ex = itg->second;
+        } else {
+            cudaGraph_t gr = nullptr;
+            BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            for (int i = 0; i < K; ++i)
+                for (BatchGroup &g : b->groups) {
+                    g.ks->rows_step(g.ptrs(), b->stream, g.count);
+                    g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, b->stream, g.count);
+                }
+            BATCH_CUDA(cudaStreamEndCapture(b->stream, &gr), "end capture");
+            cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return bfail(b, DNS2D_ERR_CUDA, "graph instantiate", e);
+            b->graphs[key] = ex;
+        }
+        BATCH_CUDA(cudaGraphLaunch(ex, b->stream), "graph launch");
+        if (E_hist || Z_hist) {
+            off = 0;
+            for (BatchGroup &g : b->groups) {
+                BATCH_CUDA(cudaMemcpyAsync(b->hist_host + (size_t)off * kChunk, g.hist, (size_t)g.count * kChunk * 16,
+                                           cudaMemcpyDeviceToHost, b->stream),
+                           "history copy");
+                off += g.count;
+            }
+            BATCH_CUDA(cudaStreamSynchronize(b->stream), "history sync");
+            off = 0;
+            for (BatchGroup &g : b->groups) {
+                for (int k = 0; k < g.count; ++k) {
+                    const int m = g.members[(size_t)k];
+                    for (int i = 0; i < K; ++i) {
+                        const double2 v = b->hist_host[(size_t)(off + k) * kChunk + i];
+                        if (E_hist) E_hist[(size_t)m * nsteps + done + i] = v.x;
+                        if (Z_hist) Z_hist[(size_t)m * nsteps + done + i] = v.y;
+                    }
+                }
+                off += g.count;
+            }
+        }
+        for (MemberScalars &c : b->sc)
+            for (int i = 0; i < K; ++i) {
+                c.it += 1;
+                const float dt_old = c.dt;
+                c.cnm1 = c.cn;
+                c.t += dt_old;
+            }
+        done += K;
+    }
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_sync(dns2d_batch *b)
+{
+    if (!b) return DNS2D_ERR_ARG;
+    BATCH_CUDA(cudaStreamSynchronize(b->stream), "sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_get_om2(dns2d_batch *b, int member, float *om2)
+{
+    if (!b || !om2 || member < 0 || member >= b->count) return DNS2D_ERR_ARG;
+    const auto [gi, k] = b->where[(size_t)member];
+    BatchGroup &g = b->groups[(size_t)gi];
+    const size_t nom = (size_t)g.N * g.H;
+    float2 *stage = nullptr;
+    BATCH_CUDA(cudaMallocAsync((void **)&stage, nom * 8, b->stream), "staging");
+    dim3 tb(32, 8), tg((g.N + 31) / 32, (g.H + 31) / 32);
+    k_transpose_c64<<<tg, tb, 0, b->stream>>>(g.om2 + (size_t)k * nom, stage, g.H, g.N);
+    BATCH_CUDA(cudaGetLastError(), "transpose");
+    BATCH_CUDA(cudaMemcpyAsync(om2, stage, nom * 8, cudaMemcpyDeviceToHost, b->stream), "om2 copy");
+    BATCH_CUDA(cudaFreeAsync(stage, b->stream), "staging free");
+    BATCH_CUDA(cudaStreamSynchronize(b->stream), "om2 sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars *o)
+{
+    if (!b || !o || member < 0 || member >= b->count) return DNS2D_ERR_ARG;
+    const auto [gi, k] = b->where[(size_t)member];
+    (void)k;
+    const BatchGroup &g = b->groups[(size_t)gi];
+    const MemberScalars &c = b->sc[(size_t)member];
+    o->N = g.N;
+    o->NX_full = g.L;
+    o->NK_full = 3 * g.N / 4 + 1;
+    o->it = c.it;
+    o->ifn = c.ifn;
+    o->Re = c.Re;
+    o->K0 = c.K0;
+    o->visc = c.visc;
+    o->t = c.t;
+    o->dt = c.dt;
+    o->cn = c.cn;
+    o->cnm1 = c.cnm1;
+    o->cflnum = c.cflnum;
+    o->cflm = c.cflm;
     return DNS2D_OK;
 }
 
@@ -1504,6 +1893,8 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     p.part = reinterpret_cast<double2 *>(base + o_part);
     p.counter = reinterpret_cast<unsigned int *>(base + o_cnt);
     p.hist = reinterpret_cast<double2 *>(base + o_hist);
+    p.s_state = p.s_work = 0;
+    p.s_part = p.s_hist = 0;
     // the array keeps the previous call's contents: rebuild twiddles, parameters and counter
     k_noalloc_twiddles<<<(unsigned)((ks->cat->total + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(base + o_tw),
                                                                                 *ks->cat);
@@ -1514,10 +1905,10 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
         static_cast<const float2 *>(om2), p.om2, N, (int)H);
     k_transpose_c64<<<dim3((unsigned)((H + 31) / 32), (unsigned)((N + 31) / 32)), tb, 0, st>>>(
         static_cast<const float2 *>(fnm1), p.fnm1, N, (int)H);
-    ks->cols_init(p, nullptr, 1, st);  // velocity of the given vorticity
+    ks->cols_init(p, nullptr, 1, st, 1);  // velocity of the given vorticity
     for (int i = 0; i < nsteps; ++i) {
-        ks->rows_step(p, st);
-        ks->cols_step(p, i == 0 ? 1 : 0, 0, st);
+        ks->rows_step(p, st, 1);
+        ks->cols_step(p, i == 0 ? 1 : 0, 0, st, 1);
     }
     k_transpose_c64<<<dim3((unsigned)((N + 31) / 32), (unsigned)((H + 31) / 32)), tb, 0, st>>>(
         p.om2, static_cast<float2 *>(om2), (int)H, N);

@@ -86,6 +86,23 @@ struct Pointers {
     double2 *part;          // per-column (E, Z) partial sums, [H]
     unsigned int *counter;  // arrival counter for the last-block reduction
     double2 *hist;          // per-step (E, Z) history
+    // batched ensembles: member m (blockIdx.y) uses its own state, work, parameter block,
+    // partials, counter and history at these strides (all 0 for a single run)
+    size_t s_state, s_work;
+    int s_part, s_hist;
+
+    __device__ __forceinline__ Pointers member(int m) const
+    {
+        Pointers q = *this;
+        q.om2 = om2 + (size_t)m * s_state;
+        q.fnm1 = fnm1 + (size_t)m * s_state;
+        q.work = work + (size_t)m * s_work;
+        q.prm = prm + (s_state ? m : 0);
+        q.part = part + (size_t)m * s_part;
+        q.counter = counter + (s_state ? m : 0);
+        q.hist = hist + (size_t)m * s_hist;
+        return q;
+    }
 };
 
 // ------------------------------------------------------------------------------------------
@@ -168,8 +185,9 @@ __device__ __forceinline__ void rows_load_pack(float2 *s, const float2 *__restri
 // Row pass of one step.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p)
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p0)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
@@ -224,8 +242,9 @@ __device__ __forceinline__ void recover_velocity(int kx, int kz, float2 om, floa
 // Column pass of one step.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p, int first, int hist_slot)
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int first, int hist_slot)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
@@ -366,8 +385,9 @@ struct TwCat {
 };
 
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p)
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
     constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3;
     constexpr int LR1 = L / R1, LR3 = L / R3;
@@ -424,8 +444,9 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p)
 }
 
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p, int first, int hist_slot)
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p0, int first, int hist_slot)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
     constexpr int LR1 = L / R1, LR3 = L / R3;
@@ -556,8 +577,9 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p, int f
 // E is still arriving; the state column is prefetched to L2.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p, int first, int hist_slot)
+__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int first, int hist_slot)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
     constexpr int LR1 = L / R1, LR3 = L / R3;
@@ -681,9 +703,10 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p, int f
 // mode 1: from om2 (already in [kx][kz] layout): velocity recovery; om2/fnm1 left unchanged.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p, const float2 *__restrict__ uw,
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p0, const float2 *__restrict__ uw,
                                                            int mode)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
@@ -725,9 +748,10 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p, const flo
 // phys[0], phys[1] ([L][L] float each) and/or reduces the CFL maximum (NEXTDT, DX = 2 pi / N).
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p, float *phys, float *cflm,
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p0, float *phys, float *cflm,
                                                                float dx)
 {
+    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
@@ -749,7 +773,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p, float
     }
     if (cflm) {
         m = block_max<NT>(m, red);
-        if (threadIdx.x == 0) atomic_max_nonneg(cflm, m);
+        if (threadIdx.x == 0) atomic_max_nonneg(cflm + blockIdx.y, m);
     }
 }
 
