@@ -160,6 +160,26 @@ int dns2d_batch_sync(dns2d_batch *b);
 int dns2d_batch_get_om2(dns2d_batch *b, int member, float *om2);
 int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars *out);
 
+/* ---- learned subgrid closure network (no counterpart in the reference) ----
+ * Periodic 3x3 CNN: `layers` convolutions, inputs (filtered vorticity, u, w), `channels` hidden
+ * channels with GELU, one output channel (the subgrid forcing).  Arrays are [B][C][H][W] float32
+ * host buffers; parameters are one flat vector (per layer: weights [Co][Ci][3][3], bias [Co]).
+ * Training runs on the device with the library's own forward, backward and Adam kernels. */
+typedef struct dns2d_cnn dns2d_cnn;
+int dns2d_cnn_create(dns2d_cnn **out, int layers, int channels, uint64_t seed, int device);
+void dns2d_cnn_destroy(dns2d_cnn *n);
+const char *dns2d_cnn_last_error(const dns2d_cnn *n);
+int dns2d_cnn_num_params(const dns2d_cnn *n);
+int dns2d_cnn_get_params(dns2d_cnn *n, float *params);
+int dns2d_cnn_set_params(dns2d_cnn *n, const float *params);
+int dns2d_cnn_forward(dns2d_cnn *n, const float *x, int B, int H, int W, float *y);
+/* mean squared error against t and its gradient with respect to every parameter */
+int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int H, int W, double *loss,
+                        float *grad);
+/* keep a training set of count samples on the device; then Adam on random minibatches */
+int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W);
+int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses);
+
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);
 /* ms[0..3], counts[0..3]: row pass, column pass, NEXTDT/CFLM, OM2PHYS+sigma */

@@ -39,6 +39,9 @@ SYMBOLS = [
     "dns2d_batch_create", "dns2d_batch_destroy", "dns2d_batch_last_error", "dns2d_batch_stream",
     "dns2d_batch_init_k4", "dns2d_batch_next_dt", "dns2d_batch_step", "dns2d_batch_sync",
     "dns2d_batch_get_om2", "dns2d_batch_get_scalars",
+    "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
+    "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
+    "dns2d_cnn_set_dataset", "dns2d_cnn_train",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -141,6 +144,16 @@ def lib():
         "dns2d_batch_sync": (C.c_int, [vp]),
         "dns2d_batch_get_om2": (C.c_int, [vp, C.c_int, fp]),
         "dns2d_batch_get_scalars": (C.c_int, [vp, C.c_int, C.POINTER(Scalars)]),
+        "dns2d_cnn_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.c_uint64, C.c_int]),
+        "dns2d_cnn_destroy": (None, [vp]),
+        "dns2d_cnn_last_error": (C.c_char_p, [vp]),
+        "dns2d_cnn_num_params": (C.c_int, [vp]),
+        "dns2d_cnn_get_params": (C.c_int, [vp, fp]),
+        "dns2d_cnn_set_params": (C.c_int, [vp, fp]),
+        "dns2d_cnn_forward": (C.c_int, [vp, fp, C.c_int, C.c_int, C.c_int, fp]),
+        "dns2d_cnn_loss_grad": (C.c_int, [vp, fp, fp, C.c_int, C.c_int, C.c_int, dp, fp]),
+        "dns2d_cnn_set_dataset": (C.c_int, [vp, fp, fp, C.c_int, C.c_int, C.c_int]),
+        "dns2d_cnn_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -415,3 +428,73 @@ def ensemble_members(counts=((128, 32), (256, 24), (512, 8)), cfl: float = 0.1):
             out.append((N, Re, K0, cfl, seed))
             seed += 1
     return out
+
+
+class CNN:
+    """The closure network (dns2d_cnn_*): periodic 3x3 CNN, 3 inputs -> 1 output."""
+
+    def __init__(self, layers: int = 6, channels: int = 32, seed: int = 0, device: int = 0):
+        self._L = lib()
+        self.layers, self.channels = layers, channels
+        self._n = C.c_void_p()
+        rc = self._L.dns2d_cnn_create(C.byref(self._n), layers, channels, seed, device)
+        if rc:
+            raise Dns2dError(f"dns2d_cnn_create: {self._L.dns2d_strerror(rc).decode()}")
+
+    def _chk(self, rc):
+        if rc:
+            raise Dns2dError(f"{self._L.dns2d_strerror(rc).decode()}: {self._L.dns2d_cnn_last_error(self._n).decode()}")
+
+    def close(self):
+        if self._n:
+            self._L.dns2d_cnn_destroy(self._n)
+            self._n = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._n
+
+    def num_params(self) -> int:
+        return self._L.dns2d_cnn_num_params(self._n)
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), dtype=np.float32)
+        self._chk(self._L.dns2d_cnn_get_params(self._n, _fp(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._chk(self._L.dns2d_cnn_set_params(self._n, _fp(p)))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        B, _, H, W = x.shape
+        y = np.zeros((B, 1, H, W), dtype=np.float32)
+        self._chk(self._L.dns2d_cnn_forward(self._n, _fp(x), B, H, W, _fp(y)))
+        return y
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        B, _, H, W = x.shape
+        loss = C.c_double(0)
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        self._chk(self._L.dns2d_cnn_loss_grad(self._n, _fp(x), _fp(t), B, H, W, C.byref(loss), _fp(g)))
+        return loss.value, g
+
+    def set_dataset(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        n, _, H, W = x.shape
+        self._chk(self._L.dns2d_cnn_set_dataset(self._n, _fp(x), _fp(t), n, H, W))
+
+    def train(self, iters: int, batch: int, lr: float, seed: int = 0) -> np.ndarray:
+        losses = np.zeros(iters)
+        self._chk(self._L.dns2d_cnn_train(self._n, iters, batch, lr, seed, _dp(losses)))
+        return losses

@@ -8,6 +8,7 @@
 // dt/cn/cnm1 through a small parameter block written by a one-thread kernel at the start of
 // every dns2d_step call, which lets one captured graph serve every segment.
 #include "dns2d_kernels.cuh"
+#include "cnn.cuh"
 #include "../../include/dns2d.h"
 
 #include <algorithm>
@@ -1797,6 +1798,324 @@ extern "C" int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars
     o->cnm1 = c.cnm1;
     o->cflnum = c.cflnum;
     o->cflm = c.cflm;
+    return DNS2D_OK;
+}
+
+// ============================================================================================
+// Learned-closure network (cnn.cuh): parameters, activations, dataset and Adam state on the
+// device; forward / backward / training driven from here.
+// ============================================================================================
+struct dns2d_cnn {
+    int layers = 0, channels = 0, device = 0, nparams = 0;
+    std::vector<int> ci, co;       // per layer
+    std::vector<size_t> woff;      // weight offset per layer (bias follows the weights)
+    cudaStream_t stream = nullptr;
+    float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr, *wflip = nullptr, *zero = nullptr;
+    std::vector<float *> z, a;     // pre-activations / activations per layer (capacity cap_elems each)
+    float *xin = nullptr, *tgt = nullptr, *gout = nullptr, *gtmp = nullptr;
+    size_t cap_elems = 0;          // per activation tensor: B * max(C, 3) * H * W
+    int capB = 0, capH = 0, capW = 0;
+    double *part = nullptr;
+    long long step = 0;
+    float *data_x = nullptr, *data_t = nullptr;  // device-resident training set
+    int data_n = 0, data_H = 0, data_W = 0;
+    std::string err;
+};
+
+namespace {
+
+int nfail(dns2d_cnn *n, int code, const char *what, cudaError_t e = cudaSuccess)
+{
+    if (n) n->err = std::string(what) + (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : "");
+    return code;
+}
+
+#define CNN_CUDA(call, what)                                                     \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) return nfail(n, DNS2D_ERR_CUDA, what, e_);        \
+    } while (0)
+
+uint64_t sm64(uint64_t &s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+int cnn_reserve(dns2d_cnn *n, int B, int H, int W)
+{
+    if (B <= n->capB && H == n->capH && W == n->capW) return DNS2D_OK;
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "sync");
+    for (float *p : n->z) cudaFree(p);
+    for (float *p : n->a) cudaFree(p);
+    cudaFree(n->xin);
+    cudaFree(n->tgt);
+    cudaFree(n->gout);
+    cudaFree(n->gtmp);
+    n->z.assign(n->layers, nullptr);
+    n->a.assign(n->layers, nullptr);
+    const size_t cap = (size_t)B * std::max(n->channels, 3) * H * W;
+    for (int l = 0; l < n->layers; ++l) {
+        CNN_CUDA(cudaMalloc((void **)&n->z[l], cap * 4), "activation alloc");
+        CNN_CUDA(cudaMalloc((void **)&n->a[l], cap * 4), "activation alloc");
+    }
+    CNN_CUDA(cudaMalloc((void **)&n->xin, (size_t)B * 3 * H * W * 4), "input alloc");
+    CNN_CUDA(cudaMalloc((void **)&n->tgt, (size_t)B * H * W * 4), "target alloc");
+    CNN_CUDA(cudaMalloc((void **)&n->gout, cap * 4), "grad alloc");
+    CNN_CUDA(cudaMalloc((void **)&n->gtmp, cap * 4), "grad alloc");
+    n->cap_elems = cap;
+    n->capB = B;
+    n->capH = H;
+    n->capW = W;
+    return DNS2D_OK;
+}
+
+void conv(dns2d_cnn *n, const float *x, const float *w, const float *b, float *y, int B, int Ci, int Co, int H, int W)
+{
+    using namespace dns2d::cnn;
+    dim3 grid((W + TILE - 1) / TILE, (H + TILE - 1) / TILE, B * ((Co + COT - 1) / COT));
+    const size_t sm = ((size_t)Ci * (TILE + 2) * (TILE + 2) + (size_t)COT * Ci * 9) * 4;
+    k_conv3x3<<<grid, dim3(TILE, TILE), sm, n->stream>>>(x, w, b, y, B, Ci, Co, H, W);
+}
+
+// forward of B images in n->xin; output (layer L-1 pre-activation) in n->z[L-1]
+int cnn_forward_dev(dns2d_cnn *n, int B, int H, int W)
+{
+    const float *in = n->xin;
+    for (int l = 0; l < n->layers; ++l) {
+        conv(n, in, n->params + n->woff[l], n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9, n->z[l], B,
+             n->ci[l], n->co[l], H, W);
+        if (l + 1 < n->layers) {
+            const size_t cnt = (size_t)B * n->co[l] * H * W;
+            dns2d::cnn::k_gelu<<<1024, 256, 0, n->stream>>>(n->z[l], n->a[l], cnt);
+            in = n->a[l];
+        }
+    }
+    CNN_CUDA(cudaGetLastError(), "cnn forward");
+    return DNS2D_OK;
+}
+
+// backward from the loss gradient in n->gout (shape of the output); fills n->grad
+int cnn_backward_dev(dns2d_cnn *n, int B, int H, int W)
+{
+    float *dz = n->gout, *other = n->gtmp;
+    for (int l = n->layers - 1; l >= 0; --l) {
+        const float *xin = (l == 0) ? n->xin : n->a[l - 1];
+        float *dw = n->grad + n->woff[l];
+        float *db = dw + (size_t)n->co[l] * n->ci[l] * 9;
+        dns2d::cnn::k_conv3x3_wgrad<<<dim3(n->ci[l], n->co[l]), 256, 0, n->stream>>>(xin, dz, dw, db, B, n->ci[l],
+                                                                                   n->co[l], H, W);
+        if (l > 0) {
+            dns2d::cnn::k_flip_weights<<<64, 256, 0, n->stream>>>(n->params + n->woff[l], n->wflip, n->ci[l], n->co[l]);
+            conv(n, dz, n->wflip, n->zero, other, B, n->co[l], n->ci[l], H, W);
+            const size_t cnt = (size_t)B * n->ci[l] * H * W;
+            dns2d::cnn::k_gelu_back<<<1024, 256, 0, n->stream>>>(n->z[l - 1], other, cnt);
+            std::swap(dz, other);
+        }
+    }
+    CNN_CUDA(cudaGetLastError(), "cnn backward");
+    return DNS2D_OK;
+}
+
+int cnn_loss(dns2d_cnn *n, int B, int H, int W, double *loss)
+{
+    const size_t cnt = (size_t)B * H * W;
+    dns2d::cnn::k_mse<<<256, 256, 0, n->stream>>>(n->z[n->layers - 1], n->tgt, n->gout, n->part, cnt);
+    CNN_CUDA(cudaGetLastError(), "mse");
+    if (loss) {
+        double h[256];
+        CNN_CUDA(cudaMemcpyAsync(h, n->part, sizeof(h), cudaMemcpyDeviceToHost, n->stream), "loss copy");
+        CNN_CUDA(cudaStreamSynchronize(n->stream), "loss sync");
+        double t = 0.0;
+        for (double v : h) t += v;
+        *loss = t / (double)cnt;
+    }
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+extern "C" void dns2d_cnn_destroy(dns2d_cnn *n)
+{
+    if (!n) return;
+    if (n->stream) cudaStreamSynchronize(n->stream);
+    for (float *p : n->z) cudaFree(p);
+    for (float *p : n->a) cudaFree(p);
+    cudaFree(n->params);
+    cudaFree(n->grad);
+    cudaFree(n->adam_m);
+    cudaFree(n->adam_v);
+    cudaFree(n->wflip);
+    cudaFree(n->zero);
+    cudaFree(n->xin);
+    cudaFree(n->tgt);
+    cudaFree(n->gout);
+    cudaFree(n->gtmp);
+    cudaFree(n->part);
+    cudaFree(n->data_x);
+    cudaFree(n->data_t);
+    if (n->stream) cudaStreamDestroy(n->stream);
+    delete n;
+}
+
+extern "C" const char *dns2d_cnn_last_error(const dns2d_cnn *n) { return n ? n->err.c_str() : "null network"; }
+
+extern "C" int dns2d_cnn_create(dns2d_cnn **out, int layers, int channels, uint64_t seed, int device)
+{
+    if (!out || layers < 2 || channels < 1 || channels > 256) return DNS2D_ERR_ARG;
+    *out = nullptr;
+    dns2d_cnn *n = new dns2d_cnn();
+    n->layers = layers;
+    n->channels = channels;
+    n->device = device;
+    auto bail = [&](int rc) {
+        dns2d_cnn_destroy(n);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+    size_t off = 0;
+    for (int l = 0; l < layers; ++l) {
+        n->ci.push_back(l == 0 ? 3 : channels);
+        n->co.push_back(l == layers - 1 ? 1 : channels);
+        n->woff.push_back(off);
+        off += (size_t)n->co[l] * n->ci[l] * 9 + n->co[l];
+    }
+    n->nparams = (int)off;
+    // He-normal weights (Box-Muller on splitmix64), zero biases; last layer scaled by 0.1
+    std::vector<float> p(off, 0.0f);
+    uint64_t st = seed;
+    for (int l = 0; l < layers; ++l) {
+        const double sd = std::sqrt(2.0 / (9.0 * n->ci[l])) * (l == layers - 1 ? 0.1 : 1.0);
+        const size_t nw = (size_t)n->co[l] * n->ci[l] * 9;
+        for (size_t i = 0; i < nw; ++i) {
+            const double u1 = ((sm64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+            const double u2 = (sm64(st) >> 11) * (1.0 / 9007199254740992.0);
+            p[n->woff[l] + i] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2));
+        }
+    }
+    size_t maxw = 0;
+    for (int l = 0; l < layers; ++l) maxw = std::max(maxw, (size_t)n->co[l] * n->ci[l] * 9);
+    if (cudaMalloc((void **)&n->params, off * 4) != cudaSuccess || cudaMalloc((void **)&n->grad, off * 4) != cudaSuccess ||
+        cudaMalloc((void **)&n->adam_m, off * 4) != cudaSuccess || cudaMalloc((void **)&n->adam_v, off * 4) != cudaSuccess ||
+        cudaMalloc((void **)&n->wflip, maxw * 4) != cudaSuccess || cudaMalloc((void **)&n->zero, 256 * 4) != cudaSuccess ||
+        cudaMalloc((void **)&n->part, 256 * 8) != cudaSuccess)
+        return bail(DNS2D_ERR_NOMEM);
+    if (cudaMemcpy(n->params, p.data(), off * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(n->adam_m, 0, off * 4) != cudaSuccess || cudaMemset(n->adam_v, 0, off * 4) != cudaSuccess ||
+        cudaMemset(n->zero, 0, 256 * 4) != cudaSuccess)
+        return bail(DNS2D_ERR_CUDA);
+    const int smax = (int)(((size_t)channels * (dns2d::cnn::TILE + 2) * (dns2d::cnn::TILE + 2) +
+                            (size_t)dns2d::cnn::COT * channels * 9) * 4);
+    if (cudaFuncSetAttribute(dns2d::cnn::k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess)
+        return bail(DNS2D_ERR_CUDA);
+    *out = n;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_num_params(const dns2d_cnn *n) { return n ? n->nparams : 0; }
+
+extern "C" int dns2d_cnn_get_params(dns2d_cnn *n, float *p)
+{
+    if (!n || !p) return DNS2D_ERR_ARG;
+    CNN_CUDA(cudaMemcpyAsync(p, n->params, (size_t)n->nparams * 4, cudaMemcpyDeviceToHost, n->stream), "params copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "params sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_set_params(dns2d_cnn *n, const float *p)
+{
+    if (!n || !p) return DNS2D_ERR_ARG;
+    CNN_CUDA(cudaMemcpyAsync(n->params, p, (size_t)n->nparams * 4, cudaMemcpyHostToDevice, n->stream), "params copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "params sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_forward(dns2d_cnn *n, const float *x, int B, int H, int W, float *y)
+{
+    if (!n || !x || !y || B <= 0 || H <= 0 || W <= 0) return DNS2D_ERR_ARG;
+    int rc = cnn_reserve(n, B, H, W);
+    if (rc) return rc;
+    CNN_CUDA(cudaMemcpyAsync(n->xin, x, (size_t)B * 3 * H * W * 4, cudaMemcpyHostToDevice, n->stream), "input copy");
+    rc = cnn_forward_dev(n, B, H, W);
+    if (rc) return rc;
+    CNN_CUDA(cudaMemcpyAsync(y, n->z[n->layers - 1], (size_t)B * H * W * 4, cudaMemcpyDeviceToHost, n->stream), "out copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "forward sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int H, int W, double *loss,
+                                   float *grad)
+{
+    if (!n || !x || !t || B <= 0) return DNS2D_ERR_ARG;
+    int rc = cnn_reserve(n, B, H, W);
+    if (rc) return rc;
+    CNN_CUDA(cudaMemcpyAsync(n->xin, x, (size_t)B * 3 * H * W * 4, cudaMemcpyHostToDevice, n->stream), "input copy");
+    CNN_CUDA(cudaMemcpyAsync(n->tgt, t, (size_t)B * H * W * 4, cudaMemcpyHostToDevice, n->stream), "target copy");
+    if ((rc = cnn_forward_dev(n, B, H, W)) || (rc = cnn_loss(n, B, H, W, loss)) || (rc = cnn_backward_dev(n, B, H, W)))
+        return rc;
+    if (grad) CNN_CUDA(cudaMemcpyAsync(grad, n->grad, (size_t)n->nparams * 4, cudaMemcpyDeviceToHost, n->stream), "grad copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "grad sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W)
+{
+    if (!n || !x || !t || count <= 0) return DNS2D_ERR_ARG;
+    cudaFree(n->data_x);
+    cudaFree(n->data_t);
+    n->data_x = n->data_t = nullptr;
+    CNN_CUDA(cudaMalloc((void **)&n->data_x, (size_t)count * 3 * H * W * 4), "dataset alloc");
+    CNN_CUDA(cudaMalloc((void **)&n->data_t, (size_t)count * H * W * 4), "dataset alloc");
+    CNN_CUDA(cudaMemcpyAsync(n->data_x, x, (size_t)count * 3 * H * W * 4, cudaMemcpyHostToDevice, n->stream), "dataset copy");
+    CNN_CUDA(cudaMemcpyAsync(n->data_t, t, (size_t)count * H * W * 4, cudaMemcpyHostToDevice, n->stream), "dataset copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "dataset sync");
+    n->data_n = count;
+    n->data_H = H;
+    n->data_W = W;
+    return DNS2D_OK;
+}
+
+// Adam iterations on minibatches drawn (without replacement within a batch) from the resident
+// dataset by splitmix64(seed); losses (nullable) receives the loss of every iteration
+extern "C" int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses)
+{
+    if (!n || iters < 0 || batch <= 0 || !n->data_n) return DNS2D_ERR_ARG;
+    const int H = n->data_H, W = n->data_W;
+    int rc = cnn_reserve(n, batch, H, W);
+    if (rc) return rc;
+    uint64_t st = seed;
+    std::vector<int> idx((size_t)n->data_n);
+    const size_t xs = (size_t)3 * H * W, ts = (size_t)H * W;
+    for (int it = 0; it < iters; ++it) {
+        for (int i = 0; i < n->data_n; ++i) idx[(size_t)i] = i;
+        for (int i = 0; i < batch && i < n->data_n; ++i) {
+            const int j = i + (int)(sm64(st) % (uint64_t)(n->data_n - i));
+            std::swap(idx[(size_t)i], idx[(size_t)j]);
+        }
+        for (int i = 0; i < batch; ++i) {
+            const int k = idx[(size_t)(i % n->data_n)];
+            CNN_CUDA(cudaMemcpyAsync(n->xin + i * xs, n->data_x + k * xs, xs * 4, cudaMemcpyDeviceToDevice, n->stream),
+                     "batch gather");
+            CNN_CUDA(cudaMemcpyAsync(n->tgt + i * ts, n->data_t + k * ts, ts * 4, cudaMemcpyDeviceToDevice, n->stream),
+                     "batch gather");
+        }
+        double loss = 0.0;
+        if ((rc = cnn_forward_dev(n, batch, H, W)) || (rc = cnn_loss(n, batch, H, W, losses ? &loss : nullptr)) ||
+            (rc = cnn_backward_dev(n, batch, H, W)))
+            return rc;
+        n->step += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.0f - (float)std::pow((double)b1, (double)n->step);
+        const float c2 = 1.0f - (float)std::pow((double)b2, (double)n->step);
+        dns2d::cnn::k_adam<<<64, 256, 0, n->stream>>>(n->params, n->grad, n->adam_m, n->adam_v, n->nparams, lr, b1, b2,
+                                                      1e-8f, c1, c2);
+        CNN_CUDA(cudaGetLastError(), "adam");
+        if (losses) losses[it] = loss;
+    }
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "train sync");
     return DNS2D_OK;
 }
 
