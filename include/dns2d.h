@@ -180,6 +180,22 @@ int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int
 int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W);
 int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses);
 
+/* Couple a trained network to a state as its subgrid closure (NULL network detaches): every
+ * dns2d_step evaluates it on (omega/s0, u/s1, w/s2) of the current field on the L x L grid and
+ * adds s3 * its output, transformed to the retained modes, to the nonlinear term.  The plain
+ * coarse step is the fallback whenever the closure would make the resolved energy rise beyond
+ * the viscous bound (unforced 2D flow only loses energy):
+ *   energy_check 0  no check;
+ *   energy_check 1  on the device, before each step: the closure is dropped for the step when its
+ *                   energy input sum w Re(conj(om/K^2) F) exceeds the viscous loss 2 nu Z
+ *                   (steps stay in captured CUDA graphs);
+ *   energy_check 2  after each step on the host: a step whose energy rose is rolled back and
+ *                   redone without the closure (one host sync per step).
+ * dns2d_closure_stats counts closed steps and fallbacks.  The network must not be used by
+ * another state or trained while attached. */
+int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int energy_check);
+int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
+
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);
 /* ms[0..3], counts[0..3]: row pass, column pass, NEXTDT/CFLM, OM2PHYS+sigma */

@@ -41,7 +41,7 @@ SYMBOLS = [
     "dns2d_batch_get_om2", "dns2d_batch_get_scalars",
     "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
-    "dns2d_cnn_set_dataset", "dns2d_cnn_train",
+    "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_stats",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -154,6 +154,8 @@ def lib():
         "dns2d_cnn_loss_grad": (C.c_int, [vp, fp, fp, C.c_int, C.c_int, C.c_int, dp, fp]),
         "dns2d_cnn_set_dataset": (C.c_int, [vp, fp, fp, C.c_int, C.c_int, C.c_int]),
         "dns2d_cnn_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, dp]),
+        "dns2d_closure_attach": (C.c_int, [vp, vp, fp, C.c_int]),
+        "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -333,6 +335,19 @@ class Solver:
 
     def load_restart(self, path: str):
         self._chk(self._L.dns2d_load_restart(self._s, path.encode()))
+
+    def attach_closure(self, net, scales, energy_check: int = 1):
+        """Couple a trained CNN (or None to detach); scales = (s_omega, s_u, s_w, s_out);
+        energy_check 0 off, 1 device-side gate (graph-captured), 2 host rollback."""
+        sc = np.ascontiguousarray(scales, dtype=np.float32)
+        self._closure_net = net  # keep the network alive while attached
+        self._chk(self._L.dns2d_closure_attach(self._s, net.handle if net is not None else None, _fp(sc),
+                                               int(energy_check)))
+
+    def closure_stats(self):
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        self._chk(self._L.dns2d_closure_stats(self._s, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def phase_timing(self, on: bool):
         self._chk(self._L.dns2d_phase_timing(self._s, int(on)))

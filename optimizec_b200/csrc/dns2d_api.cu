@@ -43,6 +43,8 @@ struct KernelSet {
     void (*rows_from_phys)(const Pointers &, const float *, cudaStream_t);
     void (*cols_scalar)(const Pointers &, float2 *, int, cudaStream_t);
     void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
+    void (*rows_fwd_scalar)(const Pointers &, const float *, float2 *, cudaStream_t);
+    void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, cudaStream_t);
 };
 
 template <int N>
@@ -72,6 +74,8 @@ struct Launch {
         if ((e = cudaFuncSetAttribute(k_rows_from_phys<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_fwd_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_fwd_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
         return cudaSuccess;
     }
     static void rows_step(const Pointers &p, cudaStream_t s, int ny)
@@ -106,10 +110,18 @@ struct Launch {
     {
         k_rows_scalar<N><<<GB, C::NTB, smB, s>>>(p, scratch, out, mm);
     }
+    static void rows_fwd_scalar(const Pointers &p, const float *f, float2 *scratch, cudaStream_t s)
+    {
+        k_rows_fwd_scalar<N><<<GB, C::NTB, smB, s>>>(p, f, scratch);
+    }
+    static void cols_fwd_scalar(const Pointers &p, const float2 *scratch, float2 *out, cudaStream_t s)
+    {
+        k_cols_fwd_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, out);
+    }
     static KernelSet make()
     {
         return KernelSet{N, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar};
+                         rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar};
     }
 };
 
@@ -341,6 +353,17 @@ struct dns2d_state {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double phase_ms[4] = {0, 0, 0, 0};
     long long phase_n[4] = {0, 0, 0, 0};
+    // learned closure (dns2d_closure_attach)
+    dns2d_cnn *cnn = nullptr;
+    float in_scale[3] = {1, 1, 1}, out_scale = 1;
+    int closure_check = 1;
+    float2 *force = nullptr, *bk_om2 = nullptr, *bk_fnm1 = nullptr, *bk_work = nullptr;
+    float *gate = nullptr;                  // device 0/1 per step (energy gate)
+    unsigned long long *gate_off = nullptr; // device count of gated-off steps
+    std::map<int, cudaGraphExec_t> closure_graphs;
+    float *closure_in = nullptr;
+    long long closure_steps = 0, closure_fallbacks = 0;
+    double closure_E = -1.0;
     std::string err;
 
     Pointers ptrs() const
@@ -354,6 +377,8 @@ struct dns2d_state {
         p.part = part;
         p.counter = counter;
         p.hist = hist;
+        p.force = nullptr;
+        p.gate = nullptr;
         p.s_state = 0;
         p.s_work = 0;
         p.s_part = 0;
@@ -539,6 +564,14 @@ extern "C" void dns2d_destroy(dns2d_state *s)
     cudaFree(s->minmax);
     cudaFree(s->sums);
     cudaFree(s->red);
+    for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(s->gate);
+    cudaFree(s->gate_off);
+    cudaFree(s->force);
+    cudaFree(s->bk_om2);
+    cudaFree(s->bk_fnm1);
+    cudaFree(s->bk_work);
+    cudaFree(s->closure_in);
     if (s->hist_host) cudaFreeHost(s->hist_host);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -889,10 +922,13 @@ int get_graph(dns2d_state *s, int first, int K, cudaGraphExec_t *out)
 
 }  // namespace
 
+static int closure_run(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist);
+
 extern "C" int dns2d_step(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist)
 {
     if (!s || nsteps < 0) return DNS2D_ERR_ARG;
     if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
+    if (s->cnn) return closure_run(s, nsteps, E_hist, Z_hist);
     int done = 0;
     while (done < nsteps) {
         const int K = std::min(kChunk, nsteps - done);
@@ -1446,6 +1482,8 @@ struct BatchGroup {
         p.part = part;
         p.counter = counter;
         p.hist = hist;
+        p.force = nullptr;
+        p.gate = nullptr;
         p.s_state = (size_t)N * H;
         p.s_work = 2 * (size_t)L * H;
         p.s_part = H;
@@ -1872,24 +1910,26 @@ int cnn_reserve(dns2d_cnn *n, int B, int H, int W)
     return DNS2D_OK;
 }
 
-void conv(dns2d_cnn *n, const float *x, const float *w, const float *b, float *y, int B, int Ci, int Co, int H, int W)
+void conv(dns2d_cnn *n, const float *x, const float *w, const float *b, float *y, int B, int Ci, int Co, int H, int W,
+          cudaStream_t st)
 {
     using namespace dns2d::cnn;
     dim3 grid((W + TILE - 1) / TILE, (H + TILE - 1) / TILE, B * ((Co + COT - 1) / COT));
     const size_t sm = ((size_t)Ci * (TILE + 2) * (TILE + 2) + (size_t)COT * Ci * 9) * 4;
-    k_conv3x3<<<grid, dim3(TILE, TILE), sm, n->stream>>>(x, w, b, y, B, Ci, Co, H, W);
+    k_conv3x3<<<grid, dim3(TILE, TILE), sm, st>>>(x, w, b, y, B, Ci, Co, H, W);
 }
 
 // forward of B images in n->xin; output (layer L-1 pre-activation) in n->z[L-1]
-int cnn_forward_dev(dns2d_cnn *n, int B, int H, int W)
+int cnn_forward_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st = nullptr)
 {
+    if (!st) st = n->stream;
     const float *in = n->xin;
     for (int l = 0; l < n->layers; ++l) {
         conv(n, in, n->params + n->woff[l], n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9, n->z[l], B,
-             n->ci[l], n->co[l], H, W);
+             n->ci[l], n->co[l], H, W, st);
         if (l + 1 < n->layers) {
             const size_t cnt = (size_t)B * n->co[l] * H * W;
-            dns2d::cnn::k_gelu<<<1024, 256, 0, n->stream>>>(n->z[l], n->a[l], cnt);
+            dns2d::cnn::k_gelu<<<1024, 256, 0, st>>>(n->z[l], n->a[l], cnt);
             in = n->a[l];
         }
     }
@@ -1909,7 +1949,7 @@ int cnn_backward_dev(dns2d_cnn *n, int B, int H, int W)
                                                                                    n->co[l], H, W);
         if (l > 0) {
             dns2d::cnn::k_flip_weights<<<64, 256, 0, n->stream>>>(n->params + n->woff[l], n->wflip, n->ci[l], n->co[l]);
-            conv(n, dz, n->wflip, n->zero, other, B, n->co[l], n->ci[l], H, W);
+            conv(n, dz, n->wflip, n->zero, other, B, n->co[l], n->ci[l], H, W, n->stream);
             const size_t cnt = (size_t)B * n->ci[l] * H * W;
             dns2d::cnn::k_gelu_back<<<1024, 256, 0, n->stream>>>(n->z[l - 1], other, cnt);
             std::swap(dz, other);
@@ -2120,6 +2160,264 @@ extern "C" int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uin
 }
 
 // ============================================================================================
+// Learned closure coupled to a state.  Every step: the state's u, w and omega on the L x L grid
+// (the CNN's inputs, divided by the input scales) -> CNN -> forcing field (times the output
+// scale) -> its retained spectrum, added to FN in the column pass.  With the energy check on, a
+// step whose energy rises (the viscous bound: unforced 2D flow can only lose energy) is redone
+// as the plain step.
+// ============================================================================================
+namespace {
+
+__global__ void k_closure_inputs(const float *phys, float *xin, size_t plane, float s_om, float s_u, float s_w)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
+        xin[i] = phys[2 * plane + i] / s_om;
+        xin[plane + i] = phys[i] / s_u;
+        xin[2 * plane + i] = phys[plane + i] / s_w;
+    }
+}
+
+__global__ void k_scale_copy(const float *in, float *out, size_t n, float sc)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = in[i] * sc;
+}
+
+// Energy gate: the forcing F changes the energy at the rate P = sum w Re(conj(om/K^2) F); the
+// resolved energy of an unforced step can only fall (dE/dt = -2 nu Z), so the closure is kept
+// for this step only when P <= 2 nu Z, otherwise the step runs as the plain coarse step.
+__global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, float *gate,
+                               unsigned long long *off)
+{
+    __shared__ double sp[256], sz[256];
+    const int H = N / 2;
+    double P = 0.0, Z = 0.0;
+    for (size_t i = threadIdx.x; i < (size_t)N * H; i += blockDim.x) {
+        const int kx = (int)(i / N), iz = (int)(i % N);
+        const int kz = (iz < H) ? iz : iz - N;
+        const double k2 = (double)kx * kx + (double)kz * kz;
+        if (k2 == 0.0) continue;
+        const double w = (kx == 0) ? 1.0 : 2.0;
+        const float2 o = om2[i], f = force[i];
+        P += w * ((double)o.x * f.x + (double)o.y * f.y) / k2;
+        Z += 0.5 * w * ((double)o.x * o.x + (double)o.y * o.y);
+    }
+    sp[threadIdx.x] = P;
+    sz[threadIdx.x] = Z;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+            sz[threadIdx.x] += sz[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const bool keep = sp[0] <= 2.0 * (double)visc * sz[0];
+        *gate = keep ? 1.0f : 0.0f;
+        if (!keep) *off += 1ULL;
+    }
+}
+
+// forcing spectrum of the current state into s->force
+int closure_forcing(dns2d_state *s)
+{
+    dns2d_cnn *n = s->cnn;
+    const int L = s->L;
+    const size_t plane = (size_t)L * L;
+    Pointers p = s->ptrs();
+    s->ks->rows_velocity(p, s->phys, nullptr, 1.0f, s->stream, 1);
+    s->ks->cols_scalar(p, s->scratch, 0, s->stream);
+    s->ks->rows_scalar(p, s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
+    k_closure_inputs<<<256, 256, 0, s->stream>>>(s->phys, n->xin, plane, s->in_scale[0], s->in_scale[1], s->in_scale[2]);
+    DNS2D_LAUNCHED("closure inputs");
+    int rc = cnn_forward_dev(n, 1, L, L, s->stream);
+    if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
+    k_scale_copy<<<256, 256, 0, s->stream>>>(n->z[n->layers - 1], s->closure_in, plane, s->out_scale);
+    DNS2D_LAUNCHED("closure output");
+    s->ks->rows_fwd_scalar(p, s->closure_in, s->scratch, s->stream);
+    s->ks->cols_fwd_scalar(p, s->scratch, s->force, s->stream);
+    DNS2D_LAUNCHED("closure transform");
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+// one closed step on the device: forcing, energy gate, row pass, column pass (capturable)
+static int closure_device_step(dns2d_state *s, int first, int slot)
+{
+    int rc = closure_forcing(s);
+    if (rc) return rc;
+    k_closure_gate<<<1, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off);
+    Pointers p = s->ptrs();
+    p.force = s->force;
+    p.gate = s->gate;
+    s->ks->rows_step(p, s->stream, 1);
+    s->ks->cols_step(p, first, slot, s->stream, 1);
+    DNS2D_LAUNCHED("closed step");
+    return DNS2D_OK;
+}
+
+static int closure_run(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist)
+{
+    const size_t nom = (size_t)s->N * s->H, nwork = 2 * (size_t)s->L * s->H;
+    if (s->closure_check != 2) {
+        // device-side energy gate; chunks of up to 128 closed steps are captured CUDA graphs
+        int done = 0;
+        while (done < nsteps) {
+            const int K = std::min(kChunk, nsteps - done);
+            const float cnm1_first = (done == 0) ? s->cnm1 : s->cn;
+            k_set_params<<<1, 1, 0, s->stream>>>(s->prm, s->dt, cnm1_first, s->cn, s->visc);
+            DNS2D_LAUNCHED("set params");
+            const int key = (done == 0 ? 1 : 0) * 1000 + K;
+            auto itg = s->closure_graphs.find(key);
+            cudaGraphExec_t ex = nullptr;
+            if (itg != s->closure_graphs.end()) {
+                ex = itg->second;
+            } else {
+                cudaGraph_t g = nullptr;
+                DNS2D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+                for (int i = 0; i < K; ++i) {
+                    int rc = closure_device_step(s, (done == 0 && i == 0) ? 1 : 0, i);
+                    if (rc) {
+                        cudaStreamEndCapture(s->stream, &g);
+                        if (g) cudaGraphDestroy(g);
+                        return rc;
+                    }
+                }
+                DNS2D_CUDA(cudaStreamEndCapture(s->stream, &g), "end capture");
+                cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return cuda_check(s, e, "graph instantiate");
+                s->closure_graphs[key] = ex;
+            }
+            DNS2D_CUDA(cudaGraphLaunch(ex, s->stream), "graph launch");
+            if (E_hist || Z_hist) {
+                DNS2D_CUDA(cudaMemcpyAsync(s->hist_host, s->hist, (size_t)K * 16, cudaMemcpyDeviceToHost, s->stream),
+                           "history copy");
+                DNS2D_CUDA(cudaStreamSynchronize(s->stream), "history sync");
+                for (int i = 0; i < K; ++i) {
+                    if (E_hist) E_hist[done + i] = s->hist_host[i].x;
+                    if (Z_hist) Z_hist[done + i] = s->hist_host[i].y;
+                }
+            }
+            for (int i = 0; i < K; ++i) {
+                s->it += 1;
+                const float dt_old = s->dt;
+                s->cnm1 = s->cn;
+                s->t += dt_old;
+            }
+            s->closure_steps += K;
+            done += K;
+        }
+        return DNS2D_OK;
+    }
+    if (s->closure_check && s->closure_E < 0.0) {
+        double E0 = 0.0;
+        int rc = dns2d_energy_enstrophy(s, &E0, nullptr);
+        if (rc) return rc;
+        s->closure_E = E0;
+    }
+    for (int i = 0; i < nsteps; ++i) {
+        const float cnm1_eff = (i == 0) ? s->cnm1 : s->cn;
+        k_set_params<<<1, 1, 0, s->stream>>>(s->prm, s->dt, cnm1_eff, s->cn, s->visc);
+        if (s->closure_check) {
+            DNS2D_CUDA(cudaMemcpyAsync(s->bk_om2, s->om2, nom * 8, cudaMemcpyDeviceToDevice, s->stream), "backup");
+            DNS2D_CUDA(cudaMemcpyAsync(s->bk_fnm1, s->fnm1, nom * 8, cudaMemcpyDeviceToDevice, s->stream), "backup");
+            DNS2D_CUDA(cudaMemcpyAsync(s->bk_work, s->work, nwork * 8, cudaMemcpyDeviceToDevice, s->stream), "backup");
+        }
+        int rc = closure_forcing(s);
+        if (rc) return rc;
+        Pointers p = s->ptrs();
+        p.force = s->force;
+        s->ks->rows_step(p, s->stream, 1);
+        s->ks->cols_step(p, 1, 0, s->stream, 1);
+        DNS2D_LAUNCHED("closure step");
+        s->closure_steps += 1;
+        double2 ez = make_double2(0.0, 0.0);
+        if (s->closure_check || E_hist || Z_hist) {
+            DNS2D_CUDA(cudaMemcpyAsync(&ez, s->hist, 16, cudaMemcpyDeviceToHost, s->stream), "energy copy");
+            DNS2D_CUDA(cudaStreamSynchronize(s->stream), "energy sync");
+        }
+        if (s->closure_check && ez.x > s->closure_E * (1.0 + 1.0e-7)) {
+            // energy rose above the viscous bound: redo this step without the closure
+            DNS2D_CUDA(cudaMemcpyAsync(s->om2, s->bk_om2, nom * 8, cudaMemcpyDeviceToDevice, s->stream), "restore");
+            DNS2D_CUDA(cudaMemcpyAsync(s->fnm1, s->bk_fnm1, nom * 8, cudaMemcpyDeviceToDevice, s->stream), "restore");
+            DNS2D_CUDA(cudaMemcpyAsync(s->work, s->bk_work, nwork * 8, cudaMemcpyDeviceToDevice, s->stream), "restore");
+            Pointers q = s->ptrs();
+            s->ks->rows_step(q, s->stream, 1);
+            s->ks->cols_step(q, 1, 0, s->stream, 1);
+            DNS2D_LAUNCHED("plain step");
+            DNS2D_CUDA(cudaMemcpyAsync(&ez, s->hist, 16, cudaMemcpyDeviceToHost, s->stream), "energy copy");
+            DNS2D_CUDA(cudaStreamSynchronize(s->stream), "energy sync");
+            s->closure_fallbacks += 1;
+        }
+        if (s->closure_check) s->closure_E = ez.x;
+        if (E_hist) E_hist[i] = ez.x;
+        if (Z_hist) Z_hist[i] = ez.y;
+        s->it += 1;
+        const float dt_old = s->dt;
+        s->cnm1 = s->cn;
+        s->t += dt_old;
+    }
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int energy_check)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    if (!n) {  // detach
+        s->cnn = nullptr;
+        return DNS2D_OK;
+    }
+    if (!scales4) return DNS2D_ERR_ARG;
+    const size_t nom = (size_t)s->N * s->H, nwork = 2 * (size_t)s->L * s->H, plane = (size_t)s->L * s->L;
+    if (!s->force) {
+        if (cudaMalloc((void **)&s->force, nom * 8) != cudaSuccess || cudaMalloc((void **)&s->bk_om2, nom * 8) != cudaSuccess ||
+            cudaMalloc((void **)&s->bk_fnm1, nom * 8) != cudaSuccess ||
+            cudaMalloc((void **)&s->bk_work, nwork * 8) != cudaSuccess ||
+            cudaMalloc((void **)&s->closure_in, plane * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(s, DNS2D_ERR_NOMEM, "closure buffers");
+        }
+    }
+    if (!s->gate) {
+        if (cudaMalloc((void **)&s->gate, 4) != cudaSuccess || cudaMalloc((void **)&s->gate_off, 8) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(s, DNS2D_ERR_NOMEM, "closure gate");
+        }
+    }
+    DNS2D_CUDA(cudaMemsetAsync(s->gate_off, 0, 8, s->stream), "gate counter");
+    for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
+    s->closure_graphs.clear();
+    int rc = cnn_reserve(n, 1, s->L, s->L);
+    if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
+    s->cnn = n;
+    for (int c = 0; c < 3; ++c) s->in_scale[c] = scales4[c];
+    s->out_scale = scales4[3];
+    s->closure_check = (energy_check < 0 || energy_check > 2) ? 1 : energy_check;
+    s->closure_E = -1.0;
+    s->closure_steps = 0;
+    s->closure_fallbacks = 0;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    if (steps) *steps = s->closure_steps;
+    if (fallbacks) {
+        unsigned long long gated = 0;
+        if (s->gate_off) {
+            DNS2D_CUDA(cudaMemcpyAsync(&gated, s->gate_off, 8, cudaMemcpyDeviceToHost, s->stream), "gate copy");
+            DNS2D_CUDA(cudaStreamSynchronize(s->stream), "gate sync");
+        }
+        *fallbacks = s->closure_fallbacks + (long long)gated;
+    }
+    return DNS2D_OK;
+}
+
+// ============================================================================================
 // Time step without device allocation.
 //
 // For callers that may not allocate device memory at all (an application that hands the solver
@@ -2212,6 +2510,8 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     p.part = reinterpret_cast<double2 *>(base + o_part);
     p.counter = reinterpret_cast<unsigned int *>(base + o_cnt);
     p.hist = reinterpret_cast<double2 *>(base + o_hist);
+    p.force = nullptr;
+    p.gate = nullptr;
     p.s_state = p.s_work = 0;
     p.s_part = p.s_hist = 0;
     // the array keeps the previous call's contents: rebuild twiddles, parameters and counter

@@ -86,6 +86,8 @@ struct Pointers {
     double2 *part;          // per-column (E, Z) partial sums, [H]
     unsigned int *counter;  // arrival counter for the last-block reduction
     double2 *hist;          // per-step (E, Z) history
+    const float2 *force;    // optional spectral forcing added to FN, [kx][kz] like om2 (closure)
+    const float *gate;      // optional 0/1 factor on the forcing, decided on the device per step
     // batched ensembles: member m (blockIdx.y) uses its own state, work, parameter block,
     // partials, counter and history at these strides (all 0 for a single run)
     size_t s_state, s_work;
@@ -101,6 +103,8 @@ struct Pointers {
         q.part = part + (size_t)m * s_part;
         q.counter = counter + (s_state ? m : 0);
         q.hist = hist + (size_t)m * s_hist;
+        q.force = force ? force + (size_t)m * s_state : nullptr;
+        q.gate = gate;
         return q;
     }
 };
@@ -282,6 +286,12 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+            if (p.force) {
+                const float g = p.gate ? *p.gate : 1.0f;
+                const float2 f = p.force[(size_t)kx * N + iz];
+                fn.x += g * f.x;
+                fn.y += g * f.y;
+            }
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;
@@ -505,6 +515,12 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p0, int 
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+            if (p.force) {
+                const float g = p.gate ? *p.gate : 1.0f;
+                const float2 f = p.force[(size_t)kx * N + iz];
+                fn.x += g * f.x;
+                fn.y += g * f.y;
+            }
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;
@@ -630,6 +646,12 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int 
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
+            if (p.force) {
+                const float g = p.gate ? *p.gate : 1.0f;
+                const float2 f = p.force[(size_t)kx * N + iz];
+                fn.x += g * f.x;
+                fn.y += g * f.y;
+            }
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;
@@ -876,6 +898,51 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_scalar(Pointers p, const f
     if (threadIdx.x == 0) s_nmn = nmn;
     const float bmx = block_max<NT>(mx, red);
     if (threadIdx.x == 0) minmax[blockIdx.x] = make_float2(-s_nmn, bmx);
+}
+
+
+// ------------------------------------------------------------------------------------------
+// Closure support: a real field on the L x L grid -> its retained spectrum F(kx,kz) in the
+// compact [kx][kz] layout, normalised like FN: F = (1/L^2) sum_x f(x) e^{-i k.x}.
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_fwd_scalar(Pointers p, const float *f, float2 *scratch)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    extern __shared__ float2 smem[];
+    const int z0 = blockIdx.x * ROWS;
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        smem[r * LP + sidx(x)] = make_float2(f[(size_t)(z0 + r) * L + x], 0.f);
+    }
+    __syncthreads();
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    const float sc = 1.0f / (float)L;
+    for (int e = threadIdx.x; e < ROWS * H; e += NT) {
+        const int r = e % ROWS, k = e / ROWS;
+        const float2 q = smem[r * LP + sidx(k)];
+        scratch[widx<L, H>(0, z0 + r, k)] = make_float2(q.x * sc, q.y * sc);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_fwd_scalar(Pointers p, const float2 *scratch, float2 *out)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
+    extern __shared__ float2 smem[];
+    const int kx = blockIdx.x;
+    for (int z = threadIdx.x; z < L; z += NT) smem[sidx(z)] = scratch[widx<L, H>(0, z, kx)];
+    __syncthreads();
+    fft_run<TwCat<N>, L, LP, false, 1, NT>(smem, p.tw, typename C::Plan{});
+    const float sc = 1.0f / (float)L;
+    for (int iz = threadIdx.x; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        const float2 v = smem[sidx(kzi)];
+        out[(size_t)kx * N + iz] = (kz == -H) ? make_float2(0.f, 0.f) : make_float2(v.x * sc, v.y * sc);
+    }
 }
 
 }  // namespace dns2d
