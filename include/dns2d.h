@@ -194,6 +194,10 @@ int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed,
  * dns2d_closure_stats counts closed steps and fallbacks.  The network must not be used by
  * another state or trained while attached. */
 int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int energy_check);
+/* The spectral forcing the attached closure adds to FN for the current state, in the compact
+ * layout of dns2d_get_fnm1 (N x N/2 complex float, [kz][kx]); a diagnostic, the state is not
+ * advanced. */
+int dns2d_closure_forcing(dns2d_state *s, float *force);
 int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
 
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */

@@ -41,7 +41,7 @@ SYMBOLS = [
     "dns2d_batch_get_om2", "dns2d_batch_get_scalars",
     "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
-    "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_stats",
+    "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -155,6 +155,7 @@ def lib():
         "dns2d_cnn_set_dataset": (C.c_int, [vp, fp, fp, C.c_int, C.c_int, C.c_int]),
         "dns2d_cnn_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, dp]),
         "dns2d_closure_attach": (C.c_int, [vp, vp, fp, C.c_int]),
+        "dns2d_closure_forcing": (C.c_int, [vp, fp]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
@@ -343,6 +344,11 @@ class Solver:
         self._closure_net = net  # keep the network alive while attached
         self._chk(self._L.dns2d_closure_attach(self._s, net.handle if net is not None else None, _fp(sc),
                                                int(energy_check)))
+
+    def closure_forcing(self) -> np.ndarray:
+        out = np.zeros((self.N, self.H), dtype=np.complex64)
+        self._chk(self._L.dns2d_closure_forcing(self._s, _fp(out.view(np.float32))))
+        return out
 
     def closure_stats(self):
         a, b = C.c_longlong(0), C.c_longlong(0)

@@ -2248,10 +2248,12 @@ static int closure_device_step(dns2d_state *s, int first, int slot)
 {
     int rc = closure_forcing(s);
     if (rc) return rc;
-    k_closure_gate<<<1, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off);
     Pointers p = s->ptrs();
     p.force = s->force;
-    p.gate = s->gate;
+    if (s->closure_check == 1) {
+        k_closure_gate<<<1, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off);
+        p.gate = s->gate;
+    }
     s->ks->rows_step(p, s->stream, 1);
     s->ks->cols_step(p, first, slot, s->stream, 1);
     DNS2D_LAUNCHED("closed step");
@@ -2400,6 +2402,18 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
     s->closure_steps = 0;
     s->closure_fallbacks = 0;
     return DNS2D_OK;
+}
+
+// forcing spectrum that the attached closure adds to FN for the current state (compact layout of
+// dns2d_get_fnm1)
+extern "C" int dns2d_closure_forcing(dns2d_state *s, float *force)
+{
+    if (!s || !force) return DNS2D_ERR_ARG;
+    if (!s->cnn) return fail(s, DNS2D_ERR_STATE, "no closure attached");
+    if (!s->initialised) return fail(s, DNS2D_ERR_STATE, "no initial condition");
+    int rc = closure_forcing(s);
+    if (rc) return rc;
+    return download_compact(s, s->force, force);
 }
 
 extern "C" int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks)
