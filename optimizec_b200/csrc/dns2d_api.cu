@@ -8,6 +8,7 @@
 // dt/cn/cnm1 through a small parameter block written by a one-thread kernel at the start of
 // every dns2d_step call, which lets one captured graph serve every segment.
 #include "dns2d_kernels.cuh"
+#include "cluster.cuh"
 #include "cnn.cuh"
 #include "../../include/dns2d.h"
 
@@ -125,12 +126,70 @@ struct Launch {
     }
 };
 
+// Sizes whose rows exceed one CTA's shared memory: every transform runs on a cluster of 4 CTAs
+// (cluster.cuh).  Grids are 4 CTAs per row / column; the closure's forward scalar transforms are
+// not provided at these sizes.
+template <int N>
+struct LaunchC {
+    using C = CfgC<N>;
+    static constexpr size_t sm1 = (size_t)C::MP * sizeof(float2);
+    static constexpr size_t sm2 = 2 * sm1;
+
+    static cudaError_t setup()
+    {
+        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_rows_step_c<N>, a, (int)sm1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_step_c<N>, a, (int)sm2)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_init_c<N>, a, (int)sm2)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_velocity_c<N>, a, (int)sm1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_from_phys_c<N>, a, (int)sm1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_scalar_c<N>, a, (int)sm1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_scalar_c<N>, a, (int)sm1)) != cudaSuccess) return e;
+        return cudaSuccess;
+    }
+    static void rows_step(const Pointers &p, cudaStream_t s, int ny)
+    {
+        k_rows_step_c<N><<<dim3(4 * C::L, ny), C::NT, sm1, s>>>(p);
+    }
+    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
+    {
+        k_cols_step_c<N><<<dim3(4 * C::H, ny), C::NT, sm2, s>>>(p, first, slot);
+    }
+    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
+    {
+        k_cols_init_c<N><<<dim3(4 * C::H, ny), C::NT, sm2, s>>>(p, uw, mode);
+    }
+    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s, int ny)
+    {
+        k_rows_velocity_c<N><<<dim3(4 * C::L, ny), C::NT, sm1, s>>>(p, phys, cflm, dx);
+    }
+    static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
+    {
+        k_rows_from_phys_c<N><<<4 * C::L, C::NT, sm1, s>>>(p, phys);
+    }
+    static void cols_scalar(const Pointers &p, float2 *scratch, int kind, cudaStream_t s)
+    {
+        k_cols_scalar_c<N><<<4 * C::H, C::NT, sm1, s>>>(p, scratch, kind);
+    }
+    static void rows_scalar(const Pointers &p, const float2 *scratch, float *out, float2 *mm, cudaStream_t s)
+    {
+        k_rows_scalar_c<N><<<4 * C::L, C::NT, sm1, s>>>(p, scratch, out, mm);
+    }
+    static KernelSet make()
+    {
+        return KernelSet{N, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
+                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr};
+    }
+};
+
 const KernelSet *kernel_set(int N)
 {
     static const KernelSet sets[] = {
         Launch<16>::make(),   Launch<32>::make(),   Launch<64>::make(),
         Launch<128>::make(),  Launch<256>::make(),  Launch<512>::make(),
         Launch<1024>::make(), Launch<2048>::make(), Launch<4096>::make(),
+        LaunchC<840>::make(), LaunchC<29400>::make(),
     };
     for (const KernelSet &k : sets)
         if (k.N == N) return &k;
@@ -835,30 +894,39 @@ extern "C" int dns2d_k4_spectrum(int N, float K0, uint64_t seed, float *om2)
     if (!om2 || N < 8 || N % 8) return DNS2D_ERR_ARG;
     const int H = N / 2;
     std::vector<double> re((size_t)N * H), im((size_t)N * H);
-    uint64_t st = seed;
-    auto next = [&]() {
-        uint64_t z = (st += 0x9E3779B97F4A7C15ULL);
-        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-        return z ^ (z >> 31);
-    };
+    // splitmix64: the i-th draw (row-major over [iz][ix]) mixes the state seed + (i+1) * gamma, so
+    // rows are generated independently (in parallel at large N) with the same values
     const double k0 = K0;
-    for (int iz = 0; iz < N; ++iz)
-        for (int ix = 0; ix < H; ++ix) {
-            const double u = (double)(next() >> 11) * (1.0 / 9007199254740992.0);
-            const double th = 2.0 * M_PI * u;
-            const int kz = (iz < H) ? iz : iz - N;
-            const double k2 = (double)ix * ix + (double)kz * kz;
-            const size_t i = (size_t)iz * H + ix;
-            if (k2 == 0.0 || kz == -H) {
-                re[i] = im[i] = 0.0;
-                continue;
+    auto rows = [&](int iz0, int iz1) {
+        for (int iz = iz0; iz < iz1; ++iz)
+            for (int ix = 0; ix < H; ++ix) {
+                const size_t i = (size_t)iz * H + ix;
+                uint64_t z = seed + (uint64_t)(i + 1) * 0x9E3779B97F4A7C15ULL;
+                z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+                z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+                z ^= z >> 31;
+                const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+                const double th = 2.0 * M_PI * u;
+                const int kz = (iz < H) ? iz : iz - N;
+                const double k2 = (double)ix * ix + (double)kz * kz;
+                if (k2 == 0.0 || kz == -H) {
+                    re[i] = im[i] = 0.0;
+                    continue;
+                }
+                const double k = std::sqrt(k2), q = k / k0;
+                const double a = std::sqrt(k * q * q * q * q * std::exp(-2.0 * q * q));
+                re[i] = a * std::cos(th);
+                im[i] = a * std::sin(th);
             }
-            const double k = std::sqrt(k2), q = k / k0;
-            const double a = std::sqrt(k * q * q * q * q * std::exp(-2.0 * q * q));
-            re[i] = a * std::cos(th);
-            im[i] = a * std::sin(th);
-        }
+    };
+    const int nth = (N >= 2048) ? (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency())) : 1;
+    if (nth == 1) {
+        rows(0, N);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; ++t) pool.emplace_back(rows, (int)((long long)N * t / nth), (int)((long long)N * (t + 1) / nth));
+        for (auto &th : pool) th.join();
+    }
     for (int iz = H + 1; iz < N; ++iz) {  // Hermitian kx = 0 column
         re[(size_t)iz * H] = re[(size_t)(N - iz) * H];
         im[(size_t)iz * H] = -im[(size_t)(N - iz) * H];
@@ -2373,6 +2441,8 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
         return DNS2D_OK;
     }
     if (!scales4) return DNS2D_ERR_ARG;
+    if (!s->ks->rows_fwd_scalar || !s->ks->cols_fwd_scalar)
+        return fail(s, DNS2D_ERR_SIZE, "no closure transforms at N=%d", s->N);
     const size_t nom = (size_t)s->N * s->H, nwork = 2 * (size_t)s->L * s->H, plane = (size_t)s->L * s->L;
     if (!s->force) {
         if (cudaMalloc((void **)&s->force, nom * 8) != cudaSuccess || cudaMalloc((void **)&s->bk_om2, nom * 8) != cudaSuccess ||

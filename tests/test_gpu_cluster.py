@@ -1,0 +1,259 @@
+"""The cluster path (every row / column transform of L = 4 M points spread over 4 CTAs with
+distributed shared memory), used where a row exceeds one CTA's shared memory (N = 29400,
+L = 44100).  N = 840 (L = 1260 = 4 x 315) runs the same kernels at a size the FP64 oracle checks
+with the tolerances of the single-CTA path; N = 29400 is checked through size-independent
+properties (energy history against the state, energy decay, restart round trip of U, W)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+NC = 840
+HARNESS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_harness")
+
+
+def P():
+    import optimizec_b200 as mod
+
+    return mod
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def _pair(N, seed=0, Re=1e4, K0=4.0, cfl=0.1):
+    om0 = O.k4_spectrum(N, K0, seed)
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_om2(om0)
+    s = P().Solver(N, Re, K0, cfl)
+    s.init_vorticity(om0)
+    c = s.next_dt()
+    return o, s, c
+
+
+def test_cluster_initial_velocity_matches_oracle():
+    o, s, cflm = _pair(NC)
+    s.velocity_phys()
+    for c in (0, 1):
+        assert rel_l2(s.phys(c).astype(np.float64), o.ur(c)) < 2e-6, c
+    assert cflm == pytest.approx(o.scalars()["cflm"], rel=1e-6)
+    assert s.scalars()["dt"] == pytest.approx(o.scalars()["dt"], rel=1e-6)
+
+
+def test_cluster_twenty_steps_match_oracle():
+    steps = 20
+    o, s, _ = _pair(NC)
+    E_ref, Z_ref, _ = o.run(steps, 1000, steps, want_diag=False)
+    E1, Z1 = s.step(1, history=True)
+    s.next_dt()
+    E2, Z2 = s.step(steps - 1, history=True)
+    s.next_dt()
+    E = np.concatenate([E1, E2])
+    Z = np.concatenate([Z1, Z2])
+    om_g, om_r = s.om2().astype(np.complex128), o.om2()
+    assert rel_l2(om_g, om_r) <= 1e-5
+    assert np.max(np.abs(E / E_ref - 1)) <= 1e-6
+    assert np.max(np.abs(Z / Z_ref - 1)) <= 1e-6
+    sg, so = s.scalars(), o.scalars()
+    assert sg["t"] == pytest.approx(so["t"], rel=1e-6)
+    assert sg["dt"] == pytest.approx(so["dt"], rel=1e-6)
+    assert sg["cn"] == pytest.approx(so["cn"], rel=1e-6)
+    Ek_g = s.shell_spectrum()
+    Ek_r = O.shell_spectrum(om_r, Ek_g.size)
+    assert np.all(np.abs(Ek_g - Ek_r) <= 1e-5 * Ek_r + 1e-10 * Ek_r.sum())
+    fg, fr = s.fnm1().astype(np.complex128), o.fnm1()
+    big = np.abs(fr) > 1e-4 * np.abs(fr).max()
+    assert rel_l2(fg[big], fr[big]) <= 1e-5
+
+
+def test_cluster_omega_phys_sigma_and_stream_function():
+    o, s, _ = _pair(NC, seed=3)
+    s.om2phys()
+    w_ref = o.omega_phys()
+    w_gpu = s.phys(2).astype(np.float64)
+    assert rel_l2(w_gpu, w_ref) < 2e-6
+    assert int(s.display_sigma(2)) == int(O.display_sigma(w_ref))
+    # stream function: psi = om / K^2 with the mean removed, against a numpy inverse transform
+    s.stream_func()
+    psi = s.phys(2).astype(np.float64)
+    N, H, L = NC, NC // 2, 3 * NC // 2
+    om = s.om2().astype(np.complex128)
+    kz = np.where(np.arange(N) < H, np.arange(N), np.arange(N) - N)[:, None]
+    kx = np.arange(H)[None, :]
+    K2 = (kx * kx + kz * kz).astype(np.float64)
+    sp = np.where(K2 > 0, om / np.where(K2 > 0, K2, 1.0), 0.0)
+    full = np.zeros((L, L // 2 + 1), dtype=np.complex128)
+    for iz in range(N):
+        full[kz[iz, 0] % L, :H] = sp[iz]
+    ref = O.inv2d(full)
+    assert rel_l2(psi, ref) < 2e-6
+
+
+def test_cluster_pao_start_matches_oracle():
+    o = O.Oracle(NC, 1e4, 10.0, 0.25)
+    stats_o, seed_o = o.init_pao()
+    s = P().Solver(NC, 1e4, 10.0, 0.25)
+    stats_g, seed_g = s.init_pao()
+    assert seed_g == seed_o
+    assert rel_l2(s.om2().astype(np.complex128), o.om2()) < 1e-6
+    assert s.next_dt() > 0
+
+
+def test_cluster_velocity_phys_round_trip():
+    _, s, _ = _pair(NC, seed=7)
+    s.velocity_phys()
+    u, w = s.phys(0).copy(), s.phys(1).copy()
+    s.set_velocity_phys(u, w)
+    s.velocity_phys()
+    assert rel_l2(s.phys(0), u) < 2e-6
+    assert rel_l2(s.phys(1), w) < 2e-6
+
+
+def _chunked_rel_l2(a, b, rows=1024):
+    num = den = 0.0
+    for i in range(0, a.shape[0], rows):
+        x = a[i:i + rows].astype(np.complex128)
+        y = b[i:i + rows].astype(np.complex128)
+        num += float(np.sum(np.abs(x - y) ** 2))
+        den += float(np.sum(np.abs(y) ** 2))
+    return (num / den) ** 0.5
+
+
+def test_cluster_n29400_energy_history_and_conservation():
+    """C5 size: k^4 start, 3 steps.  The per-step FP64 energy from the column pass equals the
+    energy of the stored field, and at Re = 1e7 the energy is conserved to FP32 rounding (the
+    viscous loss per step, ~1e-10, is below it)."""
+    N = 29400
+    s = P().Solver(N, 1e7, 4.0, 0.1)
+    s.init_k4(0)
+    E0, Z0 = s.energy_enstrophy()
+    assert E0 == pytest.approx(0.5, rel=1e-6)
+    assert s.next_dt() > 0
+    E, Z = s.step(3, history=True)
+    E3, Z3 = s.energy_enstrophy()
+    assert E[-1] == pytest.approx(E3, rel=1e-9)
+    assert Z[-1] == pytest.approx(Z3, rel=1e-9)
+    assert np.max(np.abs(E / E0 - 1.0)) < 1e-7
+    assert np.max(np.abs(Z / Z0 - 1.0)) < 1e-5
+    s.close()
+
+
+def _sparse_field(N):
+    """A few-mode vorticity field (Hermitian on kx = 0) and its nonlinear term FN by direct
+    convolution in FP64: u = sum U_p e^{ipx}, FN(k) = kx kz (uu - ww)(k) + (kz^2 - kx^2) uw(k),
+    (ab)(k) = sum_{p+q=k} A_p B_q, U = -i kz om / K^2, W = i kx om / K^2."""
+    H = N // 2
+    modes = {(1, 2): 0.8 + 0.3j, (3, -1): -0.5 + 0.7j, (2, 5): 0.4 - 0.2j, (7, 4): 0.3 + 0.1j,
+             (5, -6): -0.2 - 0.25j, (0, 3): 0.6 + 0.2j, (11, -9): 0.05 + 0.02j}
+    om0 = np.zeros((N, H), np.complex64)
+    full = {}
+    for (kx, kz), a in modes.items():
+        om0[kz % N, kx] = a
+        if kx == 0:
+            om0[(-kz) % N, 0] = np.conj(a)
+        full[(kx, kz)] = a
+        full[(-kx, -kz)] = np.conj(a)
+    U = {k: -1j * k[1] * a / (k[0] ** 2 + k[1] ** 2) for k, a in full.items()}
+    W = {k: 1j * k[0] * a / (k[0] ** 2 + k[1] ** 2) for k, a in full.items()}
+    FN = np.zeros((N, H), np.complex128)
+    acc = {}
+    for p in full:
+        for q in full:
+            k = (p[0] + q[0], p[1] + q[1])
+            t = acc.setdefault(k, [0, 0, 0])
+            t[0] += U[p] * U[q]
+            t[1] += W[p] * W[q]
+            t[2] += U[p] * W[q]
+    for (kx, kz), (uu, ww, uw) in acc.items():
+        if 0 <= kx < H and -H < kz < H:
+            FN[kz % N, kx] = kx * kz * (uu - ww) + (kz * kz - kx * kx) * uw
+    return om0, FN
+
+
+def _k2(N):
+    H = N // 2
+    kz = np.where(np.arange(N) < H, np.arange(N), np.arange(N) - N)[:, None].astype(np.float64)
+    kx = np.arange(H)[None, :].astype(np.float64)
+    return kx * kx + kz * kz
+
+
+@pytest.mark.parametrize("N", [NC, 29400])
+def test_cluster_nonlinear_term_of_sparse_field(N):
+    """FN of a 7-mode field against its direct convolution: on the 47 modes FN occupies,
+    within 2e-6 of max |FN|; elsewhere only FP32 transform rounding, which FN weights by up to
+    K^2 (2e8 at N = 29400), so it is bounded after division by K^2."""
+    om0, FN = _sparse_field(N)
+    s = P().Solver(N, 1e7, 4.0, 0.1)
+    s.init_vorticity(om0)
+    s.next_dt()
+    s.step(1)
+    f = s.fnm1().astype(np.complex128)
+    s.close()
+    sup = np.abs(FN) > 0
+    assert int(sup.sum()) == 47
+    scale = np.abs(FN).max()
+    assert np.abs(f[sup] - FN[sup]).max() <= 2e-6 * scale
+    off = np.abs(f[~sup]) / np.maximum(_k2(N)[~sup], 1.0)
+    assert off.max() <= 2e-8 * scale, off.max()
+
+
+def _band(om, n):
+    """Modes |kz| < n/2, kx < n/2 of a compact [iz][kx] spectrum, as the compact spectrum of size n
+    (the kz = -n/2 row zero)."""
+    N = om.shape[0]
+    h = n // 2
+    out = np.zeros((n, h), dtype=np.complex128)
+    out[:h] = om[:h, :h]
+    out[h + 1:] = om[N - h + 1:, :h]
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference harness not built")
+def test_cluster_n29400_matches_fp64_and_reference_cufft(tmp_path):
+    """N = 29400 (44100^2 padded grid), seeded k^4 field, 3 steps, against
+    - the FP64 oracle: the field is band-limited (its float32 modes vanish beyond |k| ~ 30), so
+      3 steps of it are resolved exactly by the oracle at N' = 512 run with the same dt / cn
+      sequence; vorticity on |k| < 256 within 2e-7 relative L2;
+    - the reference's own cuFFT path from the same field: energy history within 1e-6, and the
+      whole field within 1e-4.  FN multiplies each code's FP32 transform rounding by K^2 (up to
+      2e8 here), so modes where the field is ~0 fill with independent FP32 noise in either code;
+      the FP64 comparison above is the accuracy statement."""
+    N, Re, K0, cfl, steps, NB = 29400, 1e7, 4.0, 0.1, 3, 512
+    om0 = P().k4_spectrum(N, K0, 11)
+    f = tmp_path / "om2.bin"
+    om0.tofile(f)
+    h = subprocess.run([HARNESS, str(N), str(Re), str(K0), str(cfl), str(steps), "1000", str(f),
+                        str(tmp_path / "ref")], capture_output=True, text=True, timeout=900)
+    assert h.returncode == 0, h.stderr[-2000:]
+    E_ref = np.array([float(l.split()[2]) for l in h.stdout.splitlines() if l.startswith("STEP ")])
+    assert E_ref.size == steps
+    om_ref = np.fromfile(tmp_path / "ref.om2", dtype=np.complex64).reshape(N, N // 2)
+    os.remove(tmp_path / "ref.om2")
+    os.remove(tmp_path / "ref.fnm1")
+    s = P().Solver(N, Re, K0, cfl)
+    s.init_vorticity(om0)
+    s.next_dt()
+    d0 = s.scalars()
+    E1, _ = s.step(1, history=True)
+    s.next_dt()
+    d1 = s.scalars()
+    E2, _ = s.step(steps - 1, history=True)
+    E = np.concatenate([E1, E2])
+    om = s.om2()
+    s.close()
+    o = O.Oracle(NB, Re, K0, cfl)
+    o.init_om2(_band(om0, NB).astype(np.complex64))
+    o.run_fixed([d0["dt"], d1["dt"], d1["dt"]], [d0["cn"], d1["cn"], d1["cn"]])
+    om_64 = o.om2()
+    err_ours = rel_l2(_band(om, NB), om_64)
+    err_ref = rel_l2(_band(om_ref, NB), om_64)
+    change = rel_l2(om_64, _band(om0, NB).astype(np.complex128))
+    assert err_ours <= 2e-7, (err_ours, err_ref, change)
+    assert np.max(np.abs(E / E_ref - 1)) <= 1e-6
+    assert _chunked_rel_l2(om, om_ref) <= 1e-4
