@@ -29,23 +29,58 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-WORKLOAD = dict(N=4096, Re=1.0e5, K0=4.0, CFL=0.1, UPDATE=100, ADAPT_VISC=0, seed=0)
+# dns4096: the headline configuration.  dns29400: the large run of the reference's README
+# (mem_cuda 29400 1E7 4 41 0.1 20 0: 41 steps, its Steady FPS after 20 warm-up steps).
+WORKLOADS = {
+    "dns4096": dict(N=4096, Re=1.0e5, K0=4.0, CFL=0.1, UPDATE=100, ADAPT_VISC=0, seed=0, steps=500, warmup=100),
+    "dns29400": dict(N=29400, Re=1.0e7, K0=4.0, CFL=0.1, UPDATE=20, ADAPT_VISC=0, seed=0, steps=21, warmup=20),
+}
+WORKLOAD = dict(WORKLOADS["dns4096"])
 METRIC = "steps/s (2D vorticity DNS time step, N=4096, 6144^2 padded grid)"
+
+
+def select_workload(name: str, n: int | None):
+    global METRIC
+    WORKLOAD.clear()
+    WORKLOAD.update(WORKLOADS.get(name, WORKLOADS["dns4096"]))
+    if n:
+        WORKLOAD["N"] = n
+    N = WORKLOAD["N"]
+    METRIC = f"steps/s (2D vorticity DNS time step, N={N}, {3 * N // 2}^2 padded grid)"
+
+
+def workload_text(N: int) -> str:
+    w = WORKLOAD
+    return (f"plain DNS N={N} ({3 * N // 2}^2 padded grid), Re={w['Re']:.0e}, K0={w['K0']:g}, CFL={w['CFL']:g}, "
+            f"ADAPT_VISC=0, UPDATE={w['UPDATE']}")
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
-    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=WORKLOAD["N"])
+    ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--cpu-steps", type=int, default=3, help="FP64 oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["dns4096", "ensemble"], default="dns4096",
-                    help="ensemble: the 64-member batched configuration (32xN=128, 24xN=256, 8xN=512)")
-    return ap.parse_args()
+    ap.add_argument("--workload", choices=["dns4096", "dns29400", "ensemble"], default="dns4096",
+                    help="dns29400: N=29400 (44100^2 grid, the reference README's large run); "
+                         "ensemble: the 64-member batched configuration (32xN=128, 24xN=256, 8xN=512)")
+    a = ap.parse_args()
+    select_workload(a.workload, a.n)
+    a.n = WORKLOAD["N"]
+    if a.steps is None:
+        a.steps = WORKLOAD["steps"]
+    if a.warmup is None:
+        a.warmup = WORKLOAD["warmup"]
+    if a.workload == "dns29400":
+        # the FP64 oracle needs > 100 GB of host memory here, and a host round trip of the
+        # 7 GB state per step would dominate the e2e figure: both are reported at N=4096
+        a.no_cpu_baseline = True
+        a.no_e2e = True
+    return a
 
 
 def measured_peaks():
@@ -298,10 +333,9 @@ def main_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"plain DNS N={N} (6144^2 padded grid), Re=1e5, K0=4, CFL=0.1, "
-                               f"ADAPT_VISC=0, UPDATE={WORKLOAD['UPDATE']}, k^4 exp(-2(k/K0)^2) IC",
+        "config": {"workload": workload_text(N) + ", k^4 exp(-2(k/K0)^2) IC",
                    "N": N, "padded_grid": 3 * N // 2, "parallelism": "replicas",
-                   "l2": "inputs larger than L2 (work 12N^2 + state 8N^2 bytes = 335 MB)"},
+                   "l2": f"inputs larger than L2 (work 12N^2 + state 8N^2 bytes = {20 * N * N / 1e6:.0f} MB)"},
         "mpts_steps_per_s": round(r["value"] * N * N / 1e6, 1),
         "step_roofline": {"bytes_per_step_survey": 76 * N * N, "bytes_per_step_min": 64 * N * N,
                           "frac_survey": round(76 * N * N * steps_s / (peak * 1e9), 4),
@@ -317,6 +351,9 @@ def main_ours(args):
         line["e2e"] = r["e2e"]
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+    elif args.workload == "dns29400":
+        line["cpu_baseline"] = None
+        line["cpu_baseline_note"] = "FP64 oracle needs > 100 GB host memory at N=29400; see the N=4096 line"
     print(json.dumps(line), flush=True)
 
 
@@ -329,11 +366,11 @@ def main_reference(args):
     base = {"impl": "reference", "metric": METRIC, "unit": "steps/s", "n_gpus": 1, "steps": K,
             "warmup": W, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"plain DNS N={N} (6144^2 padded grid), Re=1e5, K0=4, CFL=0.1, "
-                                   f"ADAPT_VISC=0, UPDATE={WORKLOAD['UPDATE']}", "N": N}}
+            "config": {"workload": workload_text(N), "N": N}}
     if os.path.exists(exe):
         env = dict(os.environ, BENCH_WARMUP_STEPS=str(W))
-        cmd = [exe, str(N), "100000", "4", str(W + K), "0.1", str(WORKLOAD["UPDATE"]), "0"]
+        cmd = [exe, str(N), f"{WORKLOAD['Re']:.0E}", f"{WORKLOAD['K0']:g}", str(W + K), f"{WORKLOAD['CFL']:g}",
+               str(WORKLOAD["UPDATE"]), "0"]
         t0 = time.perf_counter()
         p = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
         wall = time.perf_counter() - t0
