@@ -66,7 +66,7 @@ struct Launch {
         if constexpr (V2) {
             if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
-            if ((e = cudaFuncSetAttribute(k_cols_step3<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
         }
         if ((e = cudaFuncSetAttribute(k_rows_step<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
@@ -86,8 +86,10 @@ struct Launch {
     }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
     {
-        // cp.async-filled columns pay off once a column is long enough (measured on B200)
-        if constexpr (V2 && N >= 4096) k_cols_step3<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        // two thread groups per column CTA pay off once a column is long enough (measured on
+        // B200: faster at N = 4096, slower at 2048)
+        if constexpr (V2 && N >= 4096)
+            k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         else if constexpr (V2) k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         else k_cols_step<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
     }

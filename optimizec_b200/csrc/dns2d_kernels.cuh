@@ -24,6 +24,17 @@
 #pragma once
 #include "fft.cuh"
 
+// L2 prefetch distances of the large-grid passes, in CTAs ahead of the current one (0 = off).
+// A row CTA brings to L2 the input of the row two waves of resident CTAs later (148 SMs x 2
+// CTAs); a column CTA the input of the column half a wave later.  Measured on B200 at N = 4096:
+// rows 0.348 -> 0.341 ms.
+#ifndef DNS2D_PF_ROWS
+#define DNS2D_PF_ROWS 296
+#endif
+#ifndef DNS2D_PF_COLS
+#define DNS2D_PF_COLS 74
+#endif
+
 namespace dns2d {
 
 // ------------------------------------------------------------------------------------------
@@ -406,11 +417,25 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
     const int j = threadIdx.x;
     const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
     const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
+#if DNS2D_PF_ROWS
+    // bring to L2 the quarter (z % 4) of the 4-row tile that the CTA about one wave later reads
+    if (z + DNS2D_PF_ROWS < L) {
+        const int t = (z + DNS2D_PF_ROWS) >> 2, part = z & 3;
+        constexpr int QB = H * 32 / 4;  // bytes of one quarter tile of one component
+        const char *b0 = reinterpret_cast<const char *>(p.work + (size_t)t * H * 4) + part * QB;
+        for (int o = j * 128; o < 2 * QB; o += C::NT * 128)
+            prefetch_l2(o < QB ? b0 + o : b0 + (size_t)L * H * 8 + (o - QB));
+    }
+#endif
     // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW
     if (j < LR1) {
         float2 v[R1];
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
+            if (slot_in_band<L, R1, H, L - H>(r)) {  // inside the zero band for every j
+                v[r] = make_float2(0.f, 0.f);
+                continue;
+            }
             const int k = j + r * LR1;
             float2 a = make_float2(0.f, 0.f), b = a;
             const bool lo = k < H, hi = k > L - H;
@@ -441,7 +466,8 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
     __syncthreads();
     if (j < LR3) sm_store<L, R3, 1>(s, v, j);
     stage1<TwCat<N>, L, R2, R3, false>(s, p.tw);
-    stage1<TwCat<N>, L, R1, R3 * R2, false>(s, p.tw);
+    // the unpack reads Q[k] and Q[L-k] for k < H: positions in [H, L-H] are never read
+    stage1_last_band<TwCat<N>, L, R1, false, H, L - H>(s, p.tw);
     __syncthreads();
     float2 *__restrict__ Do = p.work + widx<L, H>(0, z, 0);
     float2 *__restrict__ Eo = p.work + widx<L, H>(1, z, 0);
@@ -588,42 +614,109 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p0, int 
 }
 
 // ------------------------------------------------------------------------------------------
-// Column pass with asynchronous column loads: both columns (D, E) are requested with cp.async
-// at entry (no registers held by loads in flight); D's transform starts when D has landed while
-// E is still arriving; the state column is prefetched to L2.
+// Column pass with one CTA of two thread groups per column: group 0 transforms D (then U),
+// group 1 E (then W), each group synchronising on its own named barrier; the spectral update
+// uses the whole CTA.  Same arithmetic as k_cols_step2.  One 768-thread CTA per SM holds half
+// the shared memory of two 384-thread CTAs with the same number of warps, which leaves L1 room
+// for the twiddle tables (N = 4096 on B200: 0.680 -> 0.655 ms per step; no register spills at
+// 80 registers, where the single-group kernel spilled 272 bytes).  The columns arrive by
+// cp.async (no registers held by loads in flight) and the state column is prefetched to L2.
 // ------------------------------------------------------------------------------------------
+template <int NTH>
+__device__ __forceinline__ void group_sync(int id)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NTH) : "memory");
+}
+
+template <class Cat, int L, int R, int NS, bool INV, int NTH>
+__device__ __forceinline__ void stage1g(float2 *s, const float2 *tw, int j, int bar)
+{
+    constexpr int LR = L / R;
+    float2 v[R];
+    group_sync<NTH>(bar);
+    if (j < LR) {
+        sm_load<L, R>(v, s, j);
+        bfly<Cat, L, R, NS, INV>(v, j, tw);
+    }
+    group_sync<NTH>(bar);
+    if (j < LR) sm_store<L, R, NS>(s, v, j);
+}
+
+// group stage variants with a compile-time band [B0, B1]: a first stage (Ns = 1) whose inputs in
+// the band are zero, and a last stage (Ns = L/R) whose outputs in the band are never read
+template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1>
+__device__ __forceinline__ void stage1g_first_band(float2 *s, const float2 *tw, int j, int bar)
+{
+    constexpr int LR = L / R;
+    float2 v[R];
+    group_sync<NTH>(bar);
+    if (j < LR) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            v[r] = slot_in_band<L, R, B0, B1>(r) ? make_float2(0.f, 0.f) : s[sidx(j + r * LR)];
+        DFT<R, INV>::run(v);
+    }
+    group_sync<NTH>(bar);
+    if (j < LR) sm_store<L, R, 1>(s, v, j);
+}
+
+template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1>
+__device__ __forceinline__ void stage1g_last_band(float2 *s, const float2 *tw, int j, int bar)
+{
+    constexpr int LR = L / R;
+    float2 v[R];
+    group_sync<NTH>(bar);
+    if (j < LR) {
+        sm_load<L, R>(v, s, j);
+        bfly<Cat, L, R, LR, INV>(v, j, tw);
+    }
+    group_sync<NTH>(bar);
+    if (j < LR) {
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+            if (!slot_in_band<L, R, B0, B1>(q)) s[sidx(j + q * LR)] = v[q];
+    }
+}
+
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int first, int hist_slot)
+__global__ void __launch_bounds__(2 * Cfg2<N>::NT, 1) k_cols_step4(Pointers p0, int first, int hist_slot)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
-    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
-    constexpr int LR1 = L / R1, LR3 = L / R3;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, NT2 = 2 * C::NT;
+    constexpr int R1 = C::R1, R2 = C::R2, R3 = C::R3, LR1 = L / R1;
+    static_assert(NT % 32 == 0, "groups must be whole warps");
     extern __shared__ float2 smem[];
     __shared__ double2 red[32];
     __shared__ bool am_last;
     const int kx = blockIdx.x;
-    const int j = threadIdx.x;
+    const int g = (int)threadIdx.x / NT;  // 0: D / U, 1: E / W
+    const int j = (int)threadIdx.x - g * NT;
+    const int bar = 1 + g;
     float2 *sD = smem, *sE = smem + LP;
+    float2 *sg = smem + g * LP;
     float2 *om2c = p.om2 + (size_t)kx * N;
     float2 *fnc = p.fnm1 + (size_t)kx * N;
-    for (int z = j; z < L; z += NT) cp_async8(sD + sidx(z), p.work + widx<L, H>(0, z, kx));
+    for (int z = j; z < L; z += NT) cp_async8(sg + sidx(z), p.work + widx<L, H>(g, z, kx));
     cp_async_commit();
-    for (int z = j; z < L; z += NT) cp_async8(sE + sidx(z), p.work + widx<L, H>(1, z, kx));
-    cp_async_commit();
-    for (int o = j * 16; o < N; o += NT * 16) {
+    for (int o = (int)threadIdx.x * 16; o < N; o += NT2 * 16) {
         prefetch_l2(om2c + o);
         prefetch_l2(fnc + o);
     }
-    // forward transforms along z, plan (R3, R2, R1); D starts while E is still landing
-    cp_async_wait<1>();
-    stage1<TwCat<N>, L, R3, 1, false>(sD, p.tw);
-    stage1<TwCat<N>, L, R2, R3, false>(sD, p.tw);
-    stage1<TwCat<N>, L, R1, R3 * R2, false>(sD, p.tw);
+#if DNS2D_PF_COLS
+    if (kx + DNS2D_PF_COLS < (int)gridDim.x) {
+        const int kp = kx + DNS2D_PF_COLS;
+        for (int q = (int)threadIdx.x; q < 2 * (L / 4); q += NT2) {
+            const int a = q / (L / 4), gg = q - a * (L / 4);
+            prefetch_l2(p.work + (size_t)a * L * H + (((size_t)gg * H + kp) << 2));
+        }
+    }
+#endif
     cp_async_wait<0>();
-    stage1<TwCat<N>, L, R3, 1, false>(sE, p.tw);
-    stage1<TwCat<N>, L, R2, R3, false>(sE, p.tw);
-    stage1<TwCat<N>, L, R1, R3 * R2, false>(sE, p.tw);
+    stage1g<TwCat<N>, L, R3, 1, false, NT>(sg, p.tw, j, bar);
+    stage1g<TwCat<N>, L, R2, R3, false, NT>(sg, p.tw, j, bar);
+    // the update reads kz_i < H and kz_i >= L - H only: the 3/2 band [H, L-H-1] is not stored
+    stage1g_last_band<TwCat<N>, L, R1, false, NT, H, L - H - 1>(sg, p.tw, j, bar);
     __syncthreads();
 
     const StepParams prm = *p.prm;
@@ -635,7 +728,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int 
     const float divxz = (float)(1.0 / ((double)L * (double)L));
     double2 ez = make_double2(0.0, 0.0);
     const double wgt = (kx == 0) ? 0.5 : 1.0;
-    for (int iz = j; iz < N; iz += NT) {
+    for (int iz = (int)threadIdx.x; iz < N; iz += NT2) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
         const float2 d = sD[sidx(kzi)];
@@ -647,10 +740,10 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int 
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
             if (p.force) {
-                const float g = p.gate ? *p.gate : 1.0f;
+                const float gt = p.gate ? *p.gate : 1.0f;
                 const float2 f = p.force[(size_t)kx * N + iz];
-                fn.x += g * f.x;
-                fn.y += g * f.y;
+                fn.x += gt * f.x;
+                fn.y += gt * f.y;
             }
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
@@ -673,11 +766,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int 
         ez.x += wgt * pw * invK2;
         ez.y += wgt * pw;
     }
-    for (int z = H + j; z < L - H; z += NT) {
-        sD[sidx(z)] = make_float2(0.f, 0.f);
-        sE[sidx(z)] = make_float2(0.f, 0.f);
-    }
-    ez = block_sum2<NT>(ez, red);
+    ez = block_sum2<NT2>(ez, red);
     if (threadIdx.x == 0) {
         p.part[kx] = ez;
         __threadfence();
@@ -687,34 +776,32 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step3(Pointers p0, int 
     __syncthreads();
     if (am_last) {
         double2 acc = make_double2(0.0, 0.0);
-        for (int i = threadIdx.x; i < H; i += NT) {
+        for (int i = (int)threadIdx.x; i < H; i += NT2) {
             const double2 q = __ldcg(&p.part[i]);
             acc.x += q.x;
             acc.y += q.y;
         }
-        acc = block_sum2<NT>(acc, red);
+        acc = block_sum2<NT2>(acc, red);
         if (threadIdx.x == 0) {
             p.hist[hist_slot] = acc;
             *p.counter = 0u;
         }
     }
-    // inverse transforms along z, plan (R3, R2, R1), the last stage straight to global memory
-#pragma unroll 1
-    for (int a = 0; a < 2; ++a) {
-        float2 *s = a ? sE : sD;
-        stage1<TwCat<N>, L, R3, 1, true>(s, p.tw);
-        stage1<TwCat<N>, L, R2, R3, true>(s, p.tw);
-        __syncthreads();
-        if (j < LR1) {
-            float2 v[R1];
-            sm_load<L, R1>(v, s, j);
-            bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
-            static_assert(LR1 % 4 == 0, "stride");
-            constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
-            float2 *ptr = p.work + widx<L, H>(a, j, kx);
+    __syncthreads();
+    // inverse transform of this group's column, plan (R3, R2, R1), last stage straight to HBM
+    // 3/2 zero padding: the band [H, L-H-1] enters the first stage as compile-time zeros
+    stage1g_first_band<TwCat<N>, L, R3, true, NT, H, L - H - 1>(sg, p.tw, j, bar);
+    stage1g<TwCat<N>, L, R2, R3, true, NT>(sg, p.tw, j, bar);
+    group_sync<NT>(bar);
+    if (j < LR1) {
+        float2 v[R1];
+        sm_load<L, R1>(v, sg, j);
+        bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
+        static_assert(LR1 % 4 == 0, "stride");
+        constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
+        float2 *ptr = p.work + widx<L, H>(g, j, kx);
 #pragma unroll
-            for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
-        }
+        for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
     }
 }
 
