@@ -179,6 +179,10 @@ int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int
 /* keep a training set of count samples on the device; then Adam on random minibatches */
 int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W);
 int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses);
+/* The same forward on the BF16 tensor-core path: the hidden 32 -> 32 layers run as implicit GEMMs
+ * on tcgen05 (bf16 weights and activations, FP32 accumulation); the 3 -> 32 and 32 -> 1 layers in
+ * FP32.  Needs channels == 32, layers >= 3 and W % 128 == 0 (DNS2D_ERR_SIZE otherwise). */
+int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, float *y);
 
 /* Couple a trained network to a state as its subgrid closure (NULL network detaches): every
  * dns2d_step evaluates it on (omega/s0, u/s1, w/s2) of the current field on the L x L grid and
@@ -199,6 +203,9 @@ int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int
  * advanced. */
 int dns2d_closure_forcing(dns2d_state *s, float *force);
 int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
+/* 1 (default): the closure network runs on the BF16 tensor-core path where the grid allows it
+ * (L % 128 == 0, 32 channels); 0: FP32 on the SIMT pipes everywhere. */
+int dns2d_closure_tensor_cores(dns2d_state *s, int enable);
 
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);

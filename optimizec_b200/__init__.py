@@ -42,6 +42,7 @@ SYMBOLS = [
     "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
+    "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -156,6 +157,8 @@ def lib():
         "dns2d_cnn_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, dp]),
         "dns2d_closure_attach": (C.c_int, [vp, vp, fp, C.c_int]),
         "dns2d_closure_forcing": (C.c_int, [vp, fp]),
+        "dns2d_cnn_forward_tc": (C.c_int, [vp, fp, C.c_int, C.c_int, C.c_int, fp]),
+        "dns2d_closure_tensor_cores": (C.c_int, [vp, C.c_int]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
@@ -350,6 +353,9 @@ class Solver:
         self._chk(self._L.dns2d_closure_forcing(self._s, _fp(out.view(np.float32))))
         return out
 
+    def closure_tensor_cores(self, enable: bool):
+        self._chk(self._L.dns2d_closure_tensor_cores(self._s, int(enable)))
+
     def closure_stats(self):
         a, b = C.c_longlong(0), C.c_longlong(0)
         self._chk(self._L.dns2d_closure_stats(self._s, C.byref(a), C.byref(b)))
@@ -498,6 +504,14 @@ class CNN:
         B, _, H, W = x.shape
         y = np.zeros((B, 1, H, W), dtype=np.float32)
         self._chk(self._L.dns2d_cnn_forward(self._n, _fp(x), B, H, W, _fp(y)))
+        return y
+
+    def forward_tc(self, x: np.ndarray) -> np.ndarray:
+        """Forward on the BF16 tensor-core path (hidden layers on tcgen05); W % 128 == 0."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        B, _, H, W = x.shape
+        y = np.zeros((B, 1, H, W), dtype=np.float32)
+        self._chk(self._L.dns2d_cnn_forward_tc(self._n, _fp(x), B, H, W, _fp(y)))
         return y
 
     def loss_grad(self, x: np.ndarray, t: np.ndarray):

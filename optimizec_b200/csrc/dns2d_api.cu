@@ -10,6 +10,7 @@
 #include "dns2d_kernels.cuh"
 #include "cluster.cuh"
 #include "cnn.cuh"
+#include "cnn_tc.cuh"
 #include "../../include/dns2d.h"
 
 #include <algorithm>
@@ -418,8 +419,11 @@ struct dns2d_state {
     dns2d_cnn *cnn = nullptr;
     float in_scale[3] = {1, 1, 1}, out_scale = 1;
     int closure_check = 1;
+    int closure_tc = 1;  // BF16 tensor-core CNN inference where the grid allows it
     float2 *force = nullptr, *bk_om2 = nullptr, *bk_fnm1 = nullptr, *bk_work = nullptr;
     float *gate = nullptr;                  // device 0/1 per step (energy gate)
+    double2 *gate_part = nullptr;           // per-block partials of the gate reduction
+    unsigned int *gate_counter = nullptr;
     unsigned long long *gate_off = nullptr; // device count of gated-off steps
     std::map<int, cudaGraphExec_t> closure_graphs;
     float *closure_in = nullptr;
@@ -628,6 +632,8 @@ extern "C" void dns2d_destroy(dns2d_state *s)
     for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
     cudaFree(s->gate);
     cudaFree(s->gate_off);
+    cudaFree(s->gate_part);
+    cudaFree(s->gate_counter);
     cudaFree(s->force);
     cudaFree(s->bk_om2);
     cudaFree(s->bk_fnm1);
@@ -1927,6 +1933,13 @@ struct dns2d_cnn {
     long long step = 0;
     float *data_x = nullptr, *data_t = nullptr;  // device-resident training set
     int data_n = 0, data_H = 0, data_W = 0;
+    // BF16 tensor-core inference path (cnn_tc.cuh): packed hidden-layer weights, NHWC bf16
+    // activations, error flag of the bounded waits; gen counts parameter changes
+    __nv_bfloat16 *wtc = nullptr;
+    __nv_bfloat16 *act_tc[2] = {nullptr, nullptr};
+    size_t act_tc_cap = 0;
+    int *tc_err = nullptr;
+    long long gen = 0, tc_gen = -1;
     std::string err;
 };
 
@@ -2007,6 +2020,68 @@ int cnn_forward_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st = nullptr
     return DNS2D_OK;
 }
 
+// BF16 tensor-core forward: hidden layers 32 -> 32 on tcgen05 (W a multiple of 128)
+bool cnn_tc_supported(const dns2d_cnn *n, int H, int W)
+{
+    return n->channels == dns2d::cnntc::C && n->layers >= 3 && W % dns2d::cnntc::TM == 0 && H % dns2d::cnntc::TR == 0;
+}
+
+int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
+{
+    const size_t need = (size_t)B * H * W * dns2d::cnntc::C;
+    CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dns2d::cnntc::SMEM_BYTES),
+             "tc smem attribute");
+    if (!n->wtc) CNN_CUDA(cudaMalloc((void **)&n->wtc, (size_t)(n->layers - 2) * 9 * 32 * 32 * 2), "tc weights alloc");
+    if (!n->tc_err) {
+        CNN_CUDA(cudaMalloc((void **)&n->tc_err, 4), "tc flag alloc");
+        CNN_CUDA(cudaMemset(n->tc_err, 0, 4), "tc flag clear");
+    }
+    if (need > n->act_tc_cap) {
+        CNN_CUDA(cudaStreamSynchronize(n->stream), "sync");
+        cudaFree(n->act_tc[0]);
+        cudaFree(n->act_tc[1]);
+        n->act_tc[0] = n->act_tc[1] = nullptr;
+        CNN_CUDA(cudaMalloc((void **)&n->act_tc[0], need * 2), "tc activation alloc");
+        CNN_CUDA(cudaMalloc((void **)&n->act_tc[1], need * 2), "tc activation alloc");
+        n->act_tc_cap = need;
+    }
+    return DNS2D_OK;
+}
+
+// packed bf16 weights follow the parameters (repacked after set_params / train)
+int cnn_tc_prepare(dns2d_cnn *n, cudaStream_t st)
+{
+    if (n->tc_gen == n->gen) return DNS2D_OK;
+    for (int l = 1; l + 1 < n->layers; ++l)
+        dns2d::cnntc::k_pack_weights<<<36, 256, 0, st>>>(n->params + n->woff[l], n->wtc + (size_t)(l - 1) * 9 * 32 * 32);
+    CNN_CUDA(cudaGetLastError(), "tc weight pack");
+    n->tc_gen = n->gen;
+    return DNS2D_OK;
+}
+
+int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st)
+{
+    using namespace dns2d::cnntc;
+    const int L = n->layers;
+    const size_t npix = (size_t)B * H * W;
+    const int g1 = (int)std::min<size_t>((npix + 255) / 256, 148 * 8);
+    k_conv_first<<<g1, 256, 0, st>>>(n->xin, n->params + n->woff[0], n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
+                                     n->act_tc[0], B, H, W);
+    int cur = 0;
+    for (int l = 1; l + 1 < L; ++l) {
+        const float *bias = n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9;
+        k_conv_tc<<<dim3((W / TM) * (H / TR), B), NT, SMEM_BYTES, st>>>(n->act_tc[cur], n->wtc + (size_t)(l - 1) * 9 * 32 * 32,
+                                                                 bias, n->act_tc[cur ^ 1], H, W, 1, n->tc_err);
+        cur ^= 1;
+    }
+    k_conv_last<<<g1, 256, 0, st>>>(n->act_tc[cur], n->params + n->woff[L - 1],
+                                    n->params + n->woff[L - 1] + (size_t)n->co[L - 1] * n->ci[L - 1] * 9,
+                                    n->z[L - 1], B, H, W);
+    CNN_CUDA(cudaGetLastError(), "tc forward");
+    return DNS2D_OK;
+}
+
 // backward from the loss gradient in n->gout (shape of the output); fills n->grad
 int cnn_backward_dev(dns2d_cnn *n, int B, int H, int W)
 {
@@ -2066,6 +2141,10 @@ extern "C" void dns2d_cnn_destroy(dns2d_cnn *n)
     cudaFree(n->part);
     cudaFree(n->data_x);
     cudaFree(n->data_t);
+    cudaFree(n->wtc);
+    cudaFree(n->act_tc[0]);
+    cudaFree(n->act_tc[1]);
+    cudaFree(n->tc_err);
     if (n->stream) cudaStreamDestroy(n->stream);
     delete n;
 }
@@ -2140,6 +2219,7 @@ extern "C" int dns2d_cnn_set_params(dns2d_cnn *n, const float *p)
     if (!n || !p) return DNS2D_ERR_ARG;
     CNN_CUDA(cudaMemcpyAsync(n->params, p, (size_t)n->nparams * 4, cudaMemcpyHostToDevice, n->stream), "params copy");
     CNN_CUDA(cudaStreamSynchronize(n->stream), "params sync");
+    n->gen += 1;
     return DNS2D_OK;
 }
 
@@ -2153,6 +2233,25 @@ extern "C" int dns2d_cnn_forward(dns2d_cnn *n, const float *x, int B, int H, int
     if (rc) return rc;
     CNN_CUDA(cudaMemcpyAsync(y, n->z[n->layers - 1], (size_t)B * H * W * 4, cudaMemcpyDeviceToHost, n->stream), "out copy");
     CNN_CUDA(cudaStreamSynchronize(n->stream), "forward sync");
+    return DNS2D_OK;
+}
+
+// the same network on the BF16 tensor-core path (hidden layers on tcgen05); W % 128 == 0
+extern "C" int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, float *y)
+{
+    if (!n || !x || !y || B <= 0 || H <= 0 || W <= 0) return DNS2D_ERR_ARG;
+    if (!cnn_tc_supported(n, H, W))
+        return nfail(n, DNS2D_ERR_SIZE, "tensor-core path needs 32 channels, >= 3 layers, W % 128 == 0 and even H");
+    int rc = cnn_reserve(n, B, H, W);
+    if (!rc) rc = cnn_tc_reserve(n, B, H, W);
+    if (rc) return rc;
+    CNN_CUDA(cudaMemcpyAsync(n->xin, x, (size_t)B * 3 * H * W * 4, cudaMemcpyHostToDevice, n->stream), "input copy");
+    if ((rc = cnn_tc_prepare(n, n->stream)) || (rc = cnn_forward_tc_dev(n, B, H, W, n->stream))) return rc;
+    CNN_CUDA(cudaMemcpyAsync(y, n->z[n->layers - 1], (size_t)B * H * W * 4, cudaMemcpyDeviceToHost, n->stream), "out copy");
+    int flag = 0;
+    CNN_CUDA(cudaMemcpyAsync(&flag, n->tc_err, 4, cudaMemcpyDeviceToHost, n->stream), "flag copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "forward sync");
+    if (flag) return nfail(n, DNS2D_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
     return DNS2D_OK;
 }
 
@@ -2226,6 +2325,7 @@ extern "C" int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uin
         if (losses) losses[it] = loss;
     }
     CNN_CUDA(cudaStreamSynchronize(n->stream), "train sync");
+    n->gen += 1;
     return DNS2D_OK;
 }
 
@@ -2256,13 +2356,16 @@ __global__ void k_scale_copy(const float *in, float *out, size_t n, float sc)
 // Energy gate: the forcing F changes the energy at the rate P = sum w Re(conj(om/K^2) F); the
 // resolved energy of an unforced step can only fall (dE/dt = -2 nu Z), so the closure is kept
 // for this step only when P <= 2 nu Z, otherwise the step runs as the plain coarse step.
+// Grid kGateBlocks x 256: per-block partials, summed in block order by the last block to arrive.
+constexpr int kGateBlocks = 64;
 __global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, float *gate,
-                               unsigned long long *off)
+                               unsigned long long *off, double2 *part, unsigned int *counter)
 {
     __shared__ double sp[256], sz[256];
+    __shared__ bool last;
     const int H = N / 2;
     double P = 0.0, Z = 0.0;
-    for (size_t i = threadIdx.x; i < (size_t)N * H; i += blockDim.x) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)N * H; i += (size_t)gridDim.x * blockDim.x) {
         const int kx = (int)(i / N), iz = (int)(i % N);
         const int kz = (iz < H) ? iz : iz - N;
         const double k2 = (double)kx * kx + (double)kz * kz;
@@ -2283,7 +2386,20 @@ __global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, fl
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        const bool keep = sp[0] <= 2.0 * (double)visc * sz[0];
+        part[blockIdx.x] = make_double2(sp[0], sz[0]);
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double Ps = 0.0, Zs = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) {
+            const double2 q = __ldcg(&part[b]);
+            Ps += q.x;
+            Zs += q.y;
+        }
+        *counter = 0u;
+        const bool keep = Ps <= 2.0 * (double)visc * Zs;
         *gate = keep ? 1.0f : 0.0f;
         if (!keep) *off += 1ULL;
     }
@@ -2301,7 +2417,8 @@ int closure_forcing(dns2d_state *s)
     s->ks->rows_scalar(p, s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
     k_closure_inputs<<<256, 256, 0, s->stream>>>(s->phys, n->xin, plane, s->in_scale[0], s->in_scale[1], s->in_scale[2]);
     DNS2D_LAUNCHED("closure inputs");
-    int rc = cnn_forward_dev(n, 1, L, L, s->stream);
+    const bool tc = s->closure_tc && cnn_tc_supported(n, L, L);
+    int rc = tc ? cnn_forward_tc_dev(n, 1, L, L, s->stream) : cnn_forward_dev(n, 1, L, L, s->stream);
     if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
     k_scale_copy<<<256, 256, 0, s->stream>>>(n->z[n->layers - 1], s->closure_in, plane, s->out_scale);
     DNS2D_LAUNCHED("closure output");
@@ -2321,7 +2438,8 @@ static int closure_device_step(dns2d_state *s, int first, int slot)
     Pointers p = s->ptrs();
     p.force = s->force;
     if (s->closure_check == 1) {
-        k_closure_gate<<<1, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off);
+        k_closure_gate<<<kGateBlocks, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off,
+                                                          s->gate_part, s->gate_counter);
         p.gate = s->gate;
     }
     s->ks->rows_step(p, s->stream, 1);
@@ -2456,7 +2574,10 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
         }
     }
     if (!s->gate) {
-        if (cudaMalloc((void **)&s->gate, 4) != cudaSuccess || cudaMalloc((void **)&s->gate_off, 8) != cudaSuccess) {
+        if (cudaMalloc((void **)&s->gate, 4) != cudaSuccess || cudaMalloc((void **)&s->gate_off, 8) != cudaSuccess ||
+            cudaMalloc((void **)&s->gate_part, kGateBlocks * 16) != cudaSuccess ||
+            cudaMalloc((void **)&s->gate_counter, 4) != cudaSuccess ||
+            cudaMemset(s->gate_counter, 0, 4) != cudaSuccess) {
             cudaGetLastError();
             return fail(s, DNS2D_ERR_NOMEM, "closure gate");
         }
@@ -2465,6 +2586,11 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
     for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
     s->closure_graphs.clear();
     int rc = cnn_reserve(n, 1, s->L, s->L);
+    if (!rc && cnn_tc_supported(n, s->L, s->L)) {
+        rc = cnn_tc_reserve(n, 1, s->L, s->L);
+        if (!rc) rc = cnn_tc_prepare(n, n->stream);
+        if (!rc && cudaStreamSynchronize(n->stream) != cudaSuccess) rc = DNS2D_ERR_CUDA;
+    }
     if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
     s->cnn = n;
     for (int c = 0; c < 3; ++c) s->in_scale[c] = scales4[c];
@@ -2478,6 +2604,17 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
 
 // forcing spectrum that the attached closure adds to FN for the current state (compact layout of
 // dns2d_get_fnm1)
+// BF16 tensor-core inference of the attached closure network (default on where the grid allows
+// it); 0 runs the FP32 SIMT network
+extern "C" int dns2d_closure_tensor_cores(dns2d_state *s, int enable)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    s->closure_tc = enable ? 1 : 0;
+    for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
+    s->closure_graphs.clear();
+    return DNS2D_OK;
+}
+
 extern "C" int dns2d_closure_forcing(dns2d_state *s, float *force)
 {
     if (!s || !force) return DNS2D_ERR_ARG;

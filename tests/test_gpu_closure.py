@@ -165,3 +165,26 @@ def test_trained_closure_improves_coarse_run(pkg):
     assert c["shell_err_max"] < 0.5 * p["shell_err_max"], r
     assert c["enstrophy_err"] < p["enstrophy_err"], r
     net.close()
+
+
+def test_tensor_core_forcing_matches_fp32_forcing(pkg):
+    """N = 256 (L = 384): the closure runs its hidden layers on the BF16 tensor-core path by
+    default; its forcing spectrum agrees with the FP32 network's within bf16 rounding."""
+    s = pkg.Solver(256, 1e5, 4.0, 0.1)
+    s.init_k4(2)
+    s.next_dt()
+    net = pkg.CNN(6, 32, seed=4)
+    s.velocity_phys()
+    s.om2phys()
+    sc = np.array([s.phys(2).std(), s.phys(0).std(), s.phys(1).std(), 0.3], dtype=np.float32)
+    s.attach_closure(net, sc, energy_check=1)
+    F_tc = s.closure_forcing().astype(np.complex128)
+    s.closure_tensor_cores(False)
+    F_32 = s.closure_forcing().astype(np.complex128)
+    s.closure_tensor_cores(True)
+    assert np.linalg.norm(F_tc - F_32) <= 3e-2 * np.linalg.norm(F_32)
+    assert np.linalg.norm(F_tc - F_32) > 0.0  # the two paths differ (bf16), so both ran
+    s.step(10)
+    assert s.closure_stats()[0] == 10
+    s.close()
+    net.close()
