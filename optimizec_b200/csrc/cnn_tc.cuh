@@ -11,7 +11,9 @@
 // 128 bytes apart, the two K chunks one plane apart) started at another 16-byte address, so the 9
 // taps need no data movement.  The weights are staged as [tap][chunk][co][8 ci] bf16.
 // One thread issues the MMAs and commits them to an mbarrier; the 4 warps then read their 32 TMEM
-// lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.
+// lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.  The
+// last layer (32 -> 1) is the same kernel with N = 16 (15 zero weight columns) writing channel 0
+// in FP32; the first layer (3 -> 32) runs on the SIMT pipes.
 //
 // Every wait on the mbarrier is bounded: past the limit the kernel sets an error flag, skips the
 // accumulator read and still frees its tensor memory.
@@ -27,12 +29,22 @@ constexpr int C = 32;        // hidden channels (input and output of the tensor-
 constexpr int TM = 128;      // pixels per tile (MMA M)
 constexpr int TR = 2;        // image rows per CTA (one tile each, sharing the halo)
 constexpr int HW = TM + 2;   // halo width
-constexpr int PLANE = (TR + 2) * HW * 16;        // bytes of one channel-chunk plane of the halo
-constexpr int A_BYTES = 4 * PLANE;               // 33 280
-constexpr int B_BYTES = 9 * 4 * C * 16;          // 18 432: [tap][chunk][co][8]
-constexpr int SMEM_BYTES = A_BYTES + B_BYTES;    // dynamic shared memory per CTA
+// one channel-chunk plane of the halo; the 16 bytes of padding put the 4 planes on different
+// banks for the pixel-major fill
+constexpr int PLANE = (TR + 2) * HW * 16 + 16;
+constexpr int A_BYTES = 4 * PLANE;               // 33 344
 constexpr int NT = 128;                          // 4 warps = 128 TMEM lanes
-constexpr int TMEM_COLS = 32 * TR;               // one 32-column accumulator per row
+// per output width NO (32 hidden channels, or 16 for the 32 -> 1 layer: 1 channel + 15 zero
+// weight columns, the smallest MMA N): weights [tap][chunk][NO][8] bf16
+template <int NO>
+struct TcShape {
+    static constexpr int B_BYTES = 9 * 4 * NO * 16;
+    static constexpr int SMEM_BYTES = A_BYTES + B_BYTES;
+    static constexpr int TMEM_COLS = NO * TR <= 32 ? 32 : NO * TR;  // allocation: power of 2 >= 32
+    // D f32, A/B bf16, both K-major, N = NO, M = 128
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NO >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+};
 constexpr unsigned kWaitLimit = 1u << 22;        // mbarrier polls before giving up
 
 // UMMA shared-memory descriptor, K-major, no swizzle (version 1 = sm_100 format)
@@ -42,8 +54,6 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo_bytes
            ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// instruction descriptor: D f32, A/B bf16, both K-major, N = 32, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(C >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 
 // GELU of the bf16 path: the tanh form of Hendrycks and Gimpel,
 //   0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))),
@@ -60,14 +70,15 @@ __device__ __forceinline__ float gelu_f(float z)
 // periodic index in [0, n) of i in [-n, 2n)
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// weights of one 32 -> 32 layer, w[co][ci][3][3] f32 -> wtc[tap][chunk][co][8] bf16
-__global__ void k_pack_weights(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wtc)
+// weights of a 32 -> Co layer, w[co][ci][3][3] f32 -> wtc[tap][chunk][NO][8] bf16 (co >= Co zero)
+template <int NO>
+__global__ void k_pack_weights(const float *__restrict__ w, int Co, __nv_bfloat16 *__restrict__ wtc)
 {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 9 * C * C; e += gridDim.x * blockDim.x) {
-        const int t = e / (C * C), r = e % (C * C);
-        const int ch = r / (C * 8), r2 = r % (C * 8), co = r2 / 8, k = r2 % 8;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 9 * 4 * NO * 8; e += gridDim.x * blockDim.x) {
+        const int t = e / (4 * NO * 8), r = e % (4 * NO * 8);
+        const int ch = r / (NO * 8), r2 = r % (NO * 8), co = r2 / 8, k = r2 % 8;
         const int ci = ch * 8 + k;
-        wtc[e] = __float2bfloat16_rn(w[((size_t)co * C + ci) * 9 + t]);
+        wtc[e] = __float2bfloat16_rn(co < Co ? w[((size_t)co * C + ci) * 9 + t] : 0.0f);
     }
 }
 
@@ -120,58 +131,17 @@ __global__ void k_conv_first(const float *__restrict__ x, const float *__restric
     }
 }
 
-// 32 -> 1 layer (SIMT, no activation): x [B][H][W][32] bf16 -> y [B][H][W] f32
-__global__ void k_conv_last(const __nv_bfloat16 *__restrict__ x, const float *__restrict__ w, const float *__restrict__ bias,
-                            float *__restrict__ y, int B, int H, int W)
-{
-    // weights as [tap][ci]: 4 input channels in one 16-byte load
-    __shared__ __align__(16) float sw[9 * C];
-    for (int e = threadIdx.x; e < C * 9; e += blockDim.x) sw[(e % 9) * C + e / 9] = w[e];
-    __syncthreads();
-    const float4 *sw4 = reinterpret_cast<const float4 *>(sw);
-    const float b0 = bias[0];
-    const size_t npix = (size_t)B * H * W;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
-        const int b = (int)(p / ((size_t)H * W));
-        const int rr = (int)(p - (size_t)b * H * W);
-        const int yy = rr / W, xx = rr - yy * W;
-        const int xs[3] = {wrap(xx - 1, W), xx, wrap(xx + 1, W)};
-        float acc = b0;
-#pragma unroll 1
-        for (int ky = 0; ky < 3; ++ky)
-#pragma unroll
-            for (int kx = 0; kx < 3; ++kx) {
-                const int sy = wrap(yy + ky - 1, H), sx = xs[kx];
-                const uint4 *src = reinterpret_cast<const uint4 *>(x + ((((size_t)b * H + sy) * W + sx) * C));
-                const int t = ky * 3 + kx;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint4 v = src[q];
-                    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
-                    const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
-                    const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
-                    const float4 w0 = sw4[t * (C / 4) + 2 * q], w1 = sw4[t * (C / 4) + 2 * q + 1];
-                    acc = fmaf(w0.x, f0.x, acc);
-                    acc = fmaf(w0.y, f0.y, acc);
-                    acc = fmaf(w0.z, f1.x, acc);
-                    acc = fmaf(w0.w, f1.y, acc);
-                    acc = fmaf(w1.x, f2.x, acc);
-                    acc = fmaf(w1.y, f2.y, acc);
-                    acc = fmaf(w1.z, f3.x, acc);
-                    acc = fmaf(w1.w, f3.y, acc);
-                }
-            }
-        y[p] = acc;
-    }
-}
-
-// 32 -> 32 layer on the tensor cores.  Grid (W/128 * H/TR, B), 128 threads.  W % 128 == 0,
-// H % TR == 0.
+// 32 -> NO layer on the tensor cores.  Grid (W/128 * H/TR, B), 128 threads.  W % 128 == 0,
+// H % TR == 0.  NO = 32: GELU, bf16 NHWC output y; NO = 16: channel 0 only, f32 output yf
+// ([B][H][W], no activation).
+template <int NO>
 __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict__ x,
                                                 const __nv_bfloat16 *__restrict__ wtc,
                                                 const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
-                                                int H, int W, int apply_gelu, int *__restrict__ err)
+                                                float *__restrict__ yf, int H, int W, int *__restrict__ err)
 {
+    using S = TcShape<NO>;
+    constexpr int B_BYTES = S::B_BYTES, TMEM_COLS = S::TMEM_COLS;
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -183,9 +153,10 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
     const int x0 = (blockIdx.x % tiles_x) * TM;
     const size_t img = (size_t)blockIdx.y * H * W;
 
-    // halo: rows y0-1..y0+TR, pixels x0-1..x0+128 (periodic), 4 chunks of 16 bytes each
+    // halo: rows y0-1..y0+TR, pixels x0-1..x0+128 (periodic), 4 chunks of 16 bytes each; pixel-major
+    // so that a warp copies 8 whole pixels (512 contiguous bytes)
     for (int e = tid; e < (TR + 2) * HW * 4; e += NT) {
-        const int c = e / ((TR + 2) * HW), r = e - c * ((TR + 2) * HW);
+        const int r = e >> 2, c = e & 3;
         const int row = r / HW, xi = r - row * HW;
         const int sy = wrap(y0 - 1 + row, H), sx = wrap(x0 - 1 + xi, W);
         const __nv_bfloat16 *src = x + ((img + (size_t)sy * W + sx) * C + c * 8);
@@ -219,7 +190,7 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
         const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sA);
         const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
 #pragma unroll
-        for (int rr = 0; rr < TR; ++rr) {  // output row y0 + rr accumulates in columns [32 rr, 32 rr + 32)
+        for (int rr = 0; rr < TR; ++rr) {  // output row y0 + rr accumulates in columns [NO rr, NO rr + NO)
             int first = 1;
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
@@ -227,13 +198,13 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const uint64_t da = smem_desc(a0 + (2 * h) * PLANE + ((rr + dy) * HW + dx) * 16, PLANE, 128);
-                    const uint64_t db = smem_desc(b0 + (t * 4 + 2 * h) * C * 16, C * 16, 128);
+                    const uint64_t db = smem_desc(b0 + (t * 4 + 2 * h) * NO * 16, NO * 16, 128);
                     const uint32_t acc = first ? 0u : 1u;
                     asm volatile(
                         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                            tmem_d + 32u * rr),
-                        "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                            tmem_d + (uint32_t)(NO * rr)),
+                        "l"(da), "l"(db), "r"(S::IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
                     first = 0;
                 }
             }
@@ -252,36 +223,40 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (done) {
-#pragma unroll 1
-      for (int rr = 0; rr < TR; ++rr) {
-        uint32_t r[32];
-        const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + 32u * rr;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-            "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-        __align__(16) __nv_bfloat162 o[C / 2];
-#pragma unroll
-        for (int co = 0; co < C; co += 2) {
-            float a = __uint_as_float(r[co]) + bias[co];
-            float b = __uint_as_float(r[co + 1]) + bias[co + 1];
-            if (apply_gelu) {
-                a = gelu_f(a);
-                b = gelu_f(b);
-            }
-            o[co / 2] = __floats2bfloat162_rn(a, b);
-        }
         const int m = warp * 32 + lane;  // TMEM lane = pixel of the tile
-        uint4 *dst = reinterpret_cast<uint4 *>(y + (img + (size_t)(y0 + rr) * W + x0 + m) * C);
-        const uint4 *src = reinterpret_cast<const uint4 *>(o);
+#pragma unroll 1
+        for (int rr = 0; rr < TR; ++rr) {
+            const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(NO * rr);
+            const size_t pix = img + (size_t)(y0 + rr) * W + x0 + m;
+            if constexpr (NO == 32) {
+                uint32_t r[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];\n"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                      "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                      "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                __align__(16) __nv_bfloat162 o[C / 2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) dst[q] = src[q];
-      }
+                for (int co = 0; co < C; co += 2)
+                    o[co / 2] = __floats2bfloat162_rn(gelu_f(__uint_as_float(r[co]) + bias[co]),
+                                                      gelu_f(__uint_as_float(r[co + 1]) + bias[co + 1]));
+                uint4 *dst = reinterpret_cast<uint4 *>(y + pix * C);
+                const uint4 *src = reinterpret_cast<const uint4 *>(o);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = src[q];
+            } else {
+                uint32_t r0;
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(r0) : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                yf[pix] = __uint_as_float(r0) + bias[0];
+            }
+        }
     } else if (lane == 0) {
         atomicExch(err, 1);
     }

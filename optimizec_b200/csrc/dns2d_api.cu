@@ -2029,10 +2029,16 @@ bool cnn_tc_supported(const dns2d_cnn *n, int H, int W)
 int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
 {
     const size_t need = (size_t)B * H * W * dns2d::cnntc::C;
-    CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  dns2d::cnntc::SMEM_BYTES),
+    CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dns2d::cnntc::TcShape<32>::SMEM_BYTES),
              "tc smem attribute");
-    if (!n->wtc) CNN_CUDA(cudaMalloc((void **)&n->wtc, (size_t)(n->layers - 2) * 9 * 32 * 32 * 2), "tc weights alloc");
+    CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dns2d::cnntc::TcShape<16>::SMEM_BYTES),
+             "tc smem attribute");
+    // hidden layers [tap][chunk][32][8], then the last layer [tap][chunk][16][8]
+    if (!n->wtc)
+        CNN_CUDA(cudaMalloc((void **)&n->wtc, ((size_t)(n->layers - 2) * 9 * 4 * 32 * 8 + 9 * 4 * 16 * 8) * 2),
+                 "tc weights alloc");
     if (!n->tc_err) {
         CNN_CUDA(cudaMalloc((void **)&n->tc_err, 4), "tc flag alloc");
         CNN_CUDA(cudaMemset(n->tc_err, 0, 4), "tc flag clear");
@@ -2054,7 +2060,10 @@ int cnn_tc_prepare(dns2d_cnn *n, cudaStream_t st)
 {
     if (n->tc_gen == n->gen) return DNS2D_OK;
     for (int l = 1; l + 1 < n->layers; ++l)
-        dns2d::cnntc::k_pack_weights<<<36, 256, 0, st>>>(n->params + n->woff[l], n->wtc + (size_t)(l - 1) * 9 * 32 * 32);
+        dns2d::cnntc::k_pack_weights<32><<<36, 256, 0, st>>>(n->params + n->woff[l], 32,
+                                                             n->wtc + (size_t)(l - 1) * 9 * 32 * 32);
+    dns2d::cnntc::k_pack_weights<16><<<18, 256, 0, st>>>(n->params + n->woff[n->layers - 1], 1,
+                                                         n->wtc + (size_t)(n->layers - 2) * 9 * 32 * 32);
     CNN_CUDA(cudaGetLastError(), "tc weight pack");
     n->tc_gen = n->gen;
     return DNS2D_OK;
@@ -2069,15 +2078,16 @@ int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st)
     k_conv_first<<<g1, 256, 0, st>>>(n->xin, n->params + n->woff[0], n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
                                      n->act_tc[0], B, H, W);
     int cur = 0;
+    const dim3 grid((W / TM) * (H / TR), B);
     for (int l = 1; l + 1 < L; ++l) {
         const float *bias = n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9;
-        k_conv_tc<<<dim3((W / TM) * (H / TR), B), NT, SMEM_BYTES, st>>>(n->act_tc[cur], n->wtc + (size_t)(l - 1) * 9 * 32 * 32,
-                                                                 bias, n->act_tc[cur ^ 1], H, W, 1, n->tc_err);
+        k_conv_tc<32><<<grid, NT, TcShape<32>::SMEM_BYTES, st>>>(n->act_tc[cur], n->wtc + (size_t)(l - 1) * 9 * 32 * 32,
+                                                                 bias, n->act_tc[cur ^ 1], nullptr, H, W, n->tc_err);
         cur ^= 1;
     }
-    k_conv_last<<<g1, 256, 0, st>>>(n->act_tc[cur], n->params + n->woff[L - 1],
-                                    n->params + n->woff[L - 1] + (size_t)n->co[L - 1] * n->ci[L - 1] * 9,
-                                    n->z[L - 1], B, H, W);
+    k_conv_tc<16><<<grid, NT, TcShape<16>::SMEM_BYTES, st>>>(
+        n->act_tc[cur], n->wtc + (size_t)(L - 2) * 9 * 32 * 32,
+        n->params + n->woff[L - 1] + (size_t)n->co[L - 1] * n->ci[L - 1] * 9, nullptr, n->z[L - 1], H, W, n->tc_err);
     CNN_CUDA(cudaGetLastError(), "tc forward");
     return DNS2D_OK;
 }
