@@ -179,9 +179,8 @@ int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int
 /* keep a training set of count samples on the device; then Adam on random minibatches */
 int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W);
 int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses);
-/* The same forward on the BF16 tensor-core path: the 32 -> 32 and 32 -> 1 layers run as implicit
- * GEMMs on tcgen05 (bf16 weights and activations, FP32 accumulation, GELU in its tanh form); the
- * 3 -> 32 layer in FP32.  Needs channels == 32, layers >= 3 and W % 128 == 0 (DNS2D_ERR_SIZE otherwise). */
+/* The same forward on the BF16 tensor-core path: every layer runs as an implicit GEMM on tcgen05
+ * (bf16 inputs, weights and activations, FP32 accumulation, GELU in its tanh form).  Needs channels == 32, layers >= 3 and W % 128 == 0 (DNS2D_ERR_SIZE otherwise). */
 int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, float *y);
 
 /* Couple a trained network to a state as its subgrid closure (NULL network detaches): every

@@ -13,7 +13,9 @@
 // One thread issues the MMAs and commits them to an mbarrier; the 4 warps then read their 32 TMEM
 // lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.  The
 // last layer (32 -> 1) is the same kernel with N = 16 (15 zero weight columns) writing channel 0
-// in FP32; the first layer (3 -> 32) runs on the SIMT pipes.
+// in FP32 times the output scale.  The first layer (3 -> 32) builds its A operand as an im2col
+// tile in shared memory (K = 3 channels x 9 taps = 27, padded to 32) straight from the three FP32
+// input planes times their input scales: 2 MMAs per tile.
 //
 // Every wait on the mbarrier is bounded: past the limit the kernel sets an error flag, skips the
 // accumulator read and still frees its tensor memory.
@@ -82,63 +84,109 @@ __global__ void k_pack_weights(const float *__restrict__ w, int Co, __nv_bfloat1
     }
 }
 
-// 3 -> 32 layer (SIMT): x [B][3][H][W] f32 -> GELU -> y [B][H][W][32] bf16
-__global__ void k_conv_first(const float *__restrict__ x, const float *__restrict__ w, const float *__restrict__ bias,
-                             __nv_bfloat16 *__restrict__ y, int B, int H, int W)
+// ------------------------------------------------------------------------------------------
+// tcgen05 / mbarrier steps shared by the kernels (one CTA of 128 threads)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp16(void *dst, const void *src)
 {
-    // weights as [k][co] (k = ci * 9 + tap) so that 4 output channels come in one 16-byte load
-    __shared__ __align__(16) float sw[27 * C];
-    __shared__ __align__(16) float sb[C];
-    for (int e = threadIdx.x; e < C * 27; e += blockDim.x) sw[(e % 27) * C + e / 27] = w[e];
-    for (int e = threadIdx.x; e < C; e += blockDim.x) sb[e] = bias[e];
-    __syncthreads();
-    const float4 *sw4 = reinterpret_cast<const float4 *>(sw);
-    const size_t npix = (size_t)B * H * W;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
-        const int b = (int)(p / ((size_t)H * W));
-        const int rr = (int)(p - (size_t)b * H * W);
-        const int yy = rr / W, xx = rr - yy * W;
-        const int xm = wrap(xx - 1, W), xp = wrap(xx + 1, W);
-        float acc[C];
-#pragma unroll
-        for (int co = 0; co < C; ++co) acc[co] = sb[co];
-#pragma unroll 1
-        for (int k3 = 0; k3 < 9; ++k3) {  // (ci, ky); the 3 taps of a row unrolled
-            const int ci = k3 / 3, ky = k3 - 3 * ci;
-            const float *row = x + (((size_t)b * 3 + ci) * H + wrap(yy + ky - 1, H)) * W;
-            const float v3[3] = {row[xm], row[xx], row[xp]};
-#pragma unroll
-            for (int kx = 0; kx < 3; ++kx) {
-                const float v = v3[kx];
-                const float4 *wk = sw4 + (k3 * 3 + kx) * (C / 4);
-#pragma unroll
-                for (int g = 0; g < C / 4; ++g) {
-                    const float4 wv = wk[g];
-                    acc[4 * g] = fmaf(wv.x, v, acc[4 * g]);
-                    acc[4 * g + 1] = fmaf(wv.y, v, acc[4 * g + 1]);
-                    acc[4 * g + 2] = fmaf(wv.z, v, acc[4 * g + 2]);
-                    acc[4 * g + 3] = fmaf(wv.w, v, acc[4 * g + 3]);
-                }
-            }
-        }
-        __align__(16) __nv_bfloat162 o[C / 2];
-#pragma unroll
-        for (int co = 0; co < C; co += 2) o[co / 2] = __floats2bfloat162_rn(gelu_f(acc[co]), gelu_f(acc[co + 1]));
-        uint4 *dst = reinterpret_cast<uint4 *>(y + p * C);
-        const uint4 *src = reinterpret_cast<const uint4 *>(o);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dst[q] = src[q];
-    }
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr(dst)), "l"(src) : "memory");
 }
 
-// 32 -> NO layer on the tensor cores.  Grid (W/128 * H/TR, B), 128 threads.  W % 128 == 0,
-// H % TR == 0.  NO = 32: GELU, bf16 NHWC output y; NO = 16: channel 0 only, f32 output yf
+// warp 0 allocates the tensor memory, thread 0 initialises the mbarrier; then every thread makes
+// its own shared-memory writes visible to the tensor-core proxy and the CTA synchronises
+template <int COLS>
+__device__ __forceinline__ uint32_t tc_setup(uint32_t *holder, uint64_t *mbar)
+{
+    const int tid = threadIdx.x;
+    if ((tid >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(holder)),
+                     "r"(COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(mbar)), "r"(1));
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    return *holder;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(saddr(mbar))
+                 : "memory");
+}
+
+// bounded wait for phase 0 of the mbarrier; false when the limit ran out
+__device__ __forceinline__ bool mma_wait(uint64_t *mbar)
+{
+    uint32_t done = 0;
+    for (unsigned it = 0; it < kWaitLimit && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(saddr(mbar)), "r"(0u)
+            : "memory");
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    return done != 0;
+}
+
+template <int COLS>
+__device__ __forceinline__ void tc_teardown(uint32_t tmem_d)
+{
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_d), "r"(COLS));
+}
+
+// 32 accumulator columns of this warp's 32 lanes -> bias, GELU, bf16, 64-byte store of one pixel
+__device__ __forceinline__ void epilogue32(uint32_t taddr, const float *__restrict__ bias, __nv_bfloat16 *dstpix)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    __align__(16) __nv_bfloat162 o[C / 2];
+#pragma unroll
+    for (int co = 0; co < C; co += 2)
+        o[co / 2] = __floats2bfloat162_rn(gelu_f(__uint_as_float(r[co]) + bias[co]),
+                                          gelu_f(__uint_as_float(r[co + 1]) + bias[co + 1]));
+    uint4 *dst = reinterpret_cast<uint4 *>(dstpix);
+    const uint4 *src = reinterpret_cast<const uint4 *>(o);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = src[q];
+}
+
+// ------------------------------------------------------------------------------------------
+// 32 -> NO layer.  Grid (W/128 * H/TR, B), 128 threads; W % 128 == 0, H % TR == 0.
+// NO = 32: GELU, bf16 NHWC output y.  NO = 16: channel 0 times out_scale, f32 output yf
 // ([B][H][W], no activation).
+// ------------------------------------------------------------------------------------------
 template <int NO>
 __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict__ x,
                                                 const __nv_bfloat16 *__restrict__ wtc,
                                                 const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
-                                                float *__restrict__ yf, int H, int W, int *__restrict__ err)
+                                                float *__restrict__ yf, float out_scale, int H, int W,
+                                                int *__restrict__ err)
 {
     using S = TcShape<NO>;
     constexpr int B_BYTES = S::B_BYTES, TMEM_COLS = S::TMEM_COLS;
@@ -159,110 +207,138 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
         const int r = e >> 2, c = e & 3;
         const int row = r / HW, xi = r - row * HW;
         const int sy = wrap(y0 - 1 + row, H), sx = wrap(x0 - 1 + xi, W);
-        const __nv_bfloat16 *src = x + ((img + (size_t)sy * W + sx) * C + c * 8);
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sA + c * PLANE + r * 16);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+        cp16(sA + c * PLANE + r * 16, x + ((img + (size_t)sy * W + sx) * C + c * 8));
     }
-    for (int e = tid; e < B_BYTES / 16; e += NT) {
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sB + e * 16);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(wtc + (size_t)e * 8) : "memory");
-    }
+    for (int e = tid; e < B_BYTES / 16; e += NT) cp16(sB + e * 16, wtc + (size_t)e * 8);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    if (warp == 0) {
-        const uint32_t holder = (uint32_t)__cvta_generic_to_shared(&tmem_base);
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(holder), "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
-    }
-    if (tid == 0) {
-        const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb), "r"(1));
-    }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    // shared memory written by this thread (cp.async) becomes visible to the tensor-core proxy
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem_d = tmem_base;
-    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+    const uint32_t tmem_d = tc_setup<TMEM_COLS>(&tmem_base, &mbar);
 
     if (tid == 0) {
-        const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sA);
-        const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
+        const uint32_t a0 = saddr(sA), b0 = saddr(sB);
 #pragma unroll
         for (int rr = 0; rr < TR; ++rr) {  // output row y0 + rr accumulates in columns [NO rr, NO rr + NO)
-            int first = 1;
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
                 const int dy = t / 3, dx = t % 3;  // halo row (relative to rr) and pixel offset of the tap
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint64_t da = smem_desc(a0 + (2 * h) * PLANE + ((rr + dy) * HW + dx) * 16, PLANE, 128);
-                    const uint64_t db = smem_desc(b0 + (t * 4 + 2 * h) * NO * 16, NO * 16, 128);
-                    const uint32_t acc = first ? 0u : 1u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                            tmem_d + (uint32_t)(NO * rr)),
-                        "l"(da), "l"(db), "r"(S::IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-                    first = 0;
-                }
+                for (int h = 0; h < 2; ++h)
+                    mma_bf16(tmem_d + (uint32_t)(NO * rr),
+                             smem_desc(a0 + (2 * h) * PLANE + ((rr + dy) * HW + dx) * 16, PLANE, 128),
+                             smem_desc(b0 + (t * 4 + 2 * h) * NO * 16, NO * 16, 128), S::IDESC, (t | h) ? 1u : 0u);
             }
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
-                     : "memory");
+        mma_commit(&mbar);
     }
-    // bounded wait for the MMAs (phase 0)
-    uint32_t done = 0;
-    for (unsigned it = 0; it < kWaitLimit && !done; ++it) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mb), "r"(0u)
-            : "memory");
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (done) {
+    if (mma_wait(&mbar)) {
         const int m = warp * 32 + lane;  // TMEM lane = pixel of the tile
 #pragma unroll 1
         for (int rr = 0; rr < TR; ++rr) {
             const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(NO * rr);
             const size_t pix = img + (size_t)(y0 + rr) * W + x0 + m;
             if constexpr (NO == 32) {
-                uint32_t r[32];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                    "[%32];\n"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                      "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                      "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                      "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                __align__(16) __nv_bfloat162 o[C / 2];
-#pragma unroll
-                for (int co = 0; co < C; co += 2)
-                    o[co / 2] = __floats2bfloat162_rn(gelu_f(__uint_as_float(r[co]) + bias[co]),
-                                                      gelu_f(__uint_as_float(r[co + 1]) + bias[co + 1]));
-                uint4 *dst = reinterpret_cast<uint4 *>(y + pix * C);
-                const uint4 *src = reinterpret_cast<const uint4 *>(o);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) dst[q] = src[q];
+                epilogue32(taddr, bias, y + pix * C);
             } else {
                 uint32_t r0;
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(r0) : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                yf[pix] = __uint_as_float(r0) + bias[0];
+                yf[pix] = (__uint_as_float(r0) + bias[0]) * out_scale;
             }
         }
     } else if (lane == 0) {
         atomicExch(err, 1);
     }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_d), "r"(TMEM_COLS));
+    tc_teardown<TMEM_COLS>(tmem_d);
+}
+
+// ------------------------------------------------------------------------------------------
+// 3 -> 32 layer on the tensor cores: K = 27 (channel ci, tap ky, kx at k = 9 ci + 3 ky + kx),
+// padded to 32.  The inputs are three f32 planes p[c] (image b at p[c] + b * pstride) times
+// s[c]; the im2col tile of TR rows x 128 pixels is built in shared memory as 4 chunk planes of
+// [pixel][8 k] bf16.  Weights [chunk][32 co][8 k] bf16 (k >= 27 zero).  GELU, bf16 NHWC output.
+// ------------------------------------------------------------------------------------------
+struct FirstIn {
+    const float *p[3];
+    float s[3];
+    size_t pstride;
+};
+constexpr int PLANE_F = TR * TM * 16;        // bytes of one chunk plane of the im2col tile
+constexpr int B_FIRST = 4 * C * 16;          // 2 KB of weights
+constexpr int SMEM_FIRST = 4 * PLANE_F + B_FIRST;
+
+// w0[co][ci][3][3] f32 -> [chunk][co][8] bf16
+__global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wtc)
+{
+    for (int e = threadIdx.x; e < 4 * C * 8; e += blockDim.x) {
+        const int ch = e / (C * 8), r = e % (C * 8), co = r / 8, k = ch * 8 + r % 8;
+        wtc[e] = __float2bfloat16_rn(k < 27 ? w[co * 27 + k] : 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const __nv_bfloat16 *__restrict__ wtc,
+                                                      const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
+                                                      int H, int W, int *__restrict__ err)
+{
+    constexpr int COLS = C * TR;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    unsigned char *sA = sm;
+    unsigned char *sB = sm + 4 * PLANE_F;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_x = W / TM;
+    const int y0 = (blockIdx.x / tiles_x) * TR;
+    const int x0 = (blockIdx.x % tiles_x) * TM;
+    const int b = blockIdx.y;
+    for (int e = tid; e < B_FIRST / 16; e += NT) cp16(sB + e * 16, wtc + (size_t)e * 8);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // im2col: thread handles pixels tid and tid + 128 of the TR x 128 tile
+#pragma unroll
+    for (int q = 0; q < TR; ++q) {
+        const int pi = tid + q * TM;  // = rr * 128 + m
+        const int rr = pi / TM, m = pi - rr * TM;
+        const int yy = y0 + rr, xx = x0 + m;
+        const int xm = wrap(xx - 1, W), xp = wrap(xx + 1, W);
+        __align__(16) __nv_bfloat16 v[32];
+#pragma unroll
+        for (int ci = 0; ci < 3; ++ci) {
+            const float *pl = in.p[ci] + (size_t)b * in.pstride;
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const float *row = pl + (size_t)wrap(yy + ky - 1, H) * W;
+                v[ci * 9 + ky * 3 + 0] = __float2bfloat16_rn(row[xm] * in.s[ci]);
+                v[ci * 9 + ky * 3 + 1] = __float2bfloat16_rn(row[xx] * in.s[ci]);
+                v[ci * 9 + ky * 3 + 2] = __float2bfloat16_rn(row[xp] * in.s[ci]);
+            }
+        }
+#pragma unroll
+        for (int k = 27; k < 32; ++k) v[k] = __float2bfloat16_rn(0.0f);
+        const uint4 *src = reinterpret_cast<const uint4 *>(v);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) *reinterpret_cast<uint4 *>(sA + c * PLANE_F + pi * 16) = src[c];
+    }
+    const uint32_t tmem_d = tc_setup<COLS>(&tmem_base, &mbar);
+    if (tid == 0) {
+        const uint32_t a0 = saddr(sA), b0 = saddr(sB);
+        constexpr uint32_t idesc = TcShape<32>::IDESC;
+#pragma unroll
+        for (int rr = 0; rr < TR; ++rr)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                mma_bf16(tmem_d + (uint32_t)(C * rr), smem_desc(a0 + (2 * h) * PLANE_F + rr * TM * 16, PLANE_F, 128),
+                         smem_desc(b0 + (2 * h) * C * 16, C * 16, 128), idesc, h ? 1u : 0u);
+        mma_commit(&mbar);
+    }
+    if (mma_wait(&mbar)) {
+        const int m = warp * 32 + lane;
+#pragma unroll 1
+        for (int rr = 0; rr < TR; ++rr) {
+            const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(C * rr);
+            epilogue32(taddr, bias, y + (((size_t)b * H + y0 + rr) * W + x0 + m) * C);
+        }
+    } else if (lane == 0) {
+        atomicExch(err, 1);
+    }
+    tc_teardown<COLS>(tmem_d);
 }
 
 }  // namespace cnntc

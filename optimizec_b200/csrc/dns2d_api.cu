@@ -2035,9 +2035,10 @@ int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
     CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   dns2d::cnntc::TcShape<16>::SMEM_BYTES),
              "tc smem attribute");
-    // hidden layers [tap][chunk][32][8], then the last layer [tap][chunk][16][8]
+    // hidden layers [tap][chunk][32][8], the last layer [tap][chunk][16][8], the first [chunk][32][8]
     if (!n->wtc)
-        CNN_CUDA(cudaMalloc((void **)&n->wtc, ((size_t)(n->layers - 2) * 9 * 4 * 32 * 8 + 9 * 4 * 16 * 8) * 2),
+        CNN_CUDA(cudaMalloc((void **)&n->wtc,
+                            ((size_t)(n->layers - 2) * 9 * 4 * 32 * 8 + 9 * 4 * 16 * 8 + 4 * 32 * 8) * 2),
                  "tc weights alloc");
     if (!n->tc_err) {
         CNN_CUDA(cudaMalloc((void **)&n->tc_err, 4), "tc flag alloc");
@@ -2064,30 +2065,35 @@ int cnn_tc_prepare(dns2d_cnn *n, cudaStream_t st)
                                                              n->wtc + (size_t)(l - 1) * 9 * 32 * 32);
     dns2d::cnntc::k_pack_weights<16><<<18, 256, 0, st>>>(n->params + n->woff[n->layers - 1], 1,
                                                          n->wtc + (size_t)(n->layers - 2) * 9 * 32 * 32);
+    dns2d::cnntc::k_pack_first<<<1, 256, 0, st>>>(n->params + n->woff[0],
+                                                  n->wtc + (size_t)(n->layers - 2) * 9 * 32 * 32 + 9 * 4 * 16 * 8);
     CNN_CUDA(cudaGetLastError(), "tc weight pack");
     n->tc_gen = n->gen;
     return DNS2D_OK;
 }
 
-int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st)
+// inputs: three f32 planes times their scales; output: the last layer times out_scale in n->z[L-1]
+int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, const dns2d::cnntc::FirstIn &in, float out_scale,
+                       cudaStream_t st)
 {
     using namespace dns2d::cnntc;
     const int L = n->layers;
-    const size_t npix = (size_t)B * H * W;
-    const int g1 = (int)std::min<size_t>((npix + 255) / 256, 148 * 8);
-    k_conv_first<<<g1, 256, 0, st>>>(n->xin, n->params + n->woff[0], n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
-                                     n->act_tc[0], B, H, W);
-    int cur = 0;
     const dim3 grid((W / TM) * (H / TR), B);
+    const __nv_bfloat16 *w_last = n->wtc + (size_t)(L - 2) * 9 * 32 * 32;
+    const __nv_bfloat16 *w_first = w_last + 9 * 4 * 16 * 8;
+    k_conv_tc_first<<<grid, NT, SMEM_FIRST, st>>>(in, w_first, n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
+                                                  n->act_tc[0], H, W, n->tc_err);
+    int cur = 0;
     for (int l = 1; l + 1 < L; ++l) {
         const float *bias = n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9;
         k_conv_tc<32><<<grid, NT, TcShape<32>::SMEM_BYTES, st>>>(n->act_tc[cur], n->wtc + (size_t)(l - 1) * 9 * 32 * 32,
-                                                                 bias, n->act_tc[cur ^ 1], nullptr, H, W, n->tc_err);
+                                                                 bias, n->act_tc[cur ^ 1], nullptr, 1.0f, H, W,
+                                                                 n->tc_err);
         cur ^= 1;
     }
     k_conv_tc<16><<<grid, NT, TcShape<16>::SMEM_BYTES, st>>>(
-        n->act_tc[cur], n->wtc + (size_t)(L - 2) * 9 * 32 * 32,
-        n->params + n->woff[L - 1] + (size_t)n->co[L - 1] * n->ci[L - 1] * 9, nullptr, n->z[L - 1], H, W, n->tc_err);
+        n->act_tc[cur], w_last, n->params + n->woff[L - 1] + (size_t)n->co[L - 1] * n->ci[L - 1] * 9, nullptr,
+        n->z[L - 1], out_scale, H, W, n->tc_err);
     CNN_CUDA(cudaGetLastError(), "tc forward");
     return DNS2D_OK;
 }
@@ -2256,7 +2262,14 @@ extern "C" int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, 
     if (!rc) rc = cnn_tc_reserve(n, B, H, W);
     if (rc) return rc;
     CNN_CUDA(cudaMemcpyAsync(n->xin, x, (size_t)B * 3 * H * W * 4, cudaMemcpyHostToDevice, n->stream), "input copy");
-    if ((rc = cnn_tc_prepare(n, n->stream)) || (rc = cnn_forward_tc_dev(n, B, H, W, n->stream))) return rc;
+    dns2d::cnntc::FirstIn in;
+    const size_t plane = (size_t)H * W;
+    for (int c = 0; c < 3; ++c) {
+        in.p[c] = n->xin + c * plane;
+        in.s[c] = 1.0f;
+    }
+    in.pstride = 3 * plane;
+    if ((rc = cnn_tc_prepare(n, n->stream)) || (rc = cnn_forward_tc_dev(n, B, H, W, in, 1.0f, n->stream))) return rc;
     CNN_CUDA(cudaMemcpyAsync(y, n->z[n->layers - 1], (size_t)B * H * W * 4, cudaMemcpyDeviceToHost, n->stream), "out copy");
     int flag = 0;
     CNN_CUDA(cudaMemcpyAsync(&flag, n->tc_err, 4, cudaMemcpyDeviceToHost, n->stream), "flag copy");
@@ -2425,14 +2438,29 @@ int closure_forcing(dns2d_state *s)
     s->ks->rows_velocity(p, s->phys, nullptr, 1.0f, s->stream, 1);
     s->ks->cols_scalar(p, s->scratch, 0, s->stream);
     s->ks->rows_scalar(p, s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
-    k_closure_inputs<<<256, 256, 0, s->stream>>>(s->phys, n->xin, plane, s->in_scale[0], s->in_scale[1], s->in_scale[2]);
-    DNS2D_LAUNCHED("closure inputs");
-    const bool tc = s->closure_tc && cnn_tc_supported(n, L, L);
-    int rc = tc ? cnn_forward_tc_dev(n, 1, L, L, s->stream) : cnn_forward_dev(n, 1, L, L, s->stream);
-    if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
-    k_scale_copy<<<256, 256, 0, s->stream>>>(n->z[n->layers - 1], s->closure_in, plane, s->out_scale);
-    DNS2D_LAUNCHED("closure output");
-    s->ks->rows_fwd_scalar(p, s->closure_in, s->scratch, s->stream);
+    const float *forcing_field = s->closure_in;
+    if (s->closure_tc && cnn_tc_supported(n, L, L)) {
+        // tensor-core path: the first layer reads (omega, u, w) / scales straight from the planes,
+        // the last layer writes its output times the output scale
+        dns2d::cnntc::FirstIn in;
+        in.p[0] = s->phys + 2 * plane;
+        in.p[1] = s->phys;
+        in.p[2] = s->phys + plane;
+        for (int c = 0; c < 3; ++c) in.s[c] = 1.0f / s->in_scale[c];
+        in.pstride = 0;
+        int rc = cnn_forward_tc_dev(n, 1, L, L, in, s->out_scale, s->stream);
+        if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
+        forcing_field = n->z[n->layers - 1];
+    } else {
+        k_closure_inputs<<<256, 256, 0, s->stream>>>(s->phys, n->xin, plane, s->in_scale[0], s->in_scale[1],
+                                                     s->in_scale[2]);
+        DNS2D_LAUNCHED("closure inputs");
+        int rc = cnn_forward_dev(n, 1, L, L, s->stream);
+        if (rc) return fail(s, rc, "closure network: %s", n->err.c_str());
+        k_scale_copy<<<256, 256, 0, s->stream>>>(n->z[n->layers - 1], s->closure_in, plane, s->out_scale);
+        DNS2D_LAUNCHED("closure output");
+    }
+    s->ks->rows_fwd_scalar(p, forcing_field, s->scratch, s->stream);
     s->ks->cols_fwd_scalar(p, s->scratch, s->force, s->stream);
     DNS2D_LAUNCHED("closure transform");
     return DNS2D_OK;

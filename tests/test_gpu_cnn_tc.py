@@ -1,8 +1,7 @@
 """BF16 tensor-core (tcgen05) forward of the closure network against the FP64 restatement with
-the same bf16 roundings (weights of every layer after the first and every hidden activation
-rounded to bf16, round to nearest even; exact erf GELU), and against the FP32 network.  The
-32 -> 32 and 32 -> 1 layers run as implicit GEMMs on the tensor cores with FP32 accumulation and
-the tanh form of GELU; the 3 -> 32 layer in FP32."""
+the same bf16 roundings (inputs, weights and every hidden activation rounded to bf16, round to
+nearest even; exact erf GELU), and against the FP32 network.  Every layer runs as an implicit
+GEMM on the tensor cores with FP32 accumulation and the tanh form of GELU."""
 import numpy as np
 import pytest
 
@@ -25,10 +24,9 @@ def bf16(a):
 
 def forward_bf16(params, layers, x):
     ps = CO.unpack(params, layers, 32)
-    a = x.astype(np.float64)
+    a = bf16(x)
     for l, (w, b) in enumerate(ps):
-        if l > 0:
-            w = bf16(w)
+        w = bf16(w)
         z = CO.conv3x3(a, w, b)
         a = bf16(CO.gelu(z)) if l < layers - 1 else z
     return a
