@@ -171,3 +171,50 @@ def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine
                      "shell_err_mean": float(rel.mean()), "enstrophy_err": abs(Z / Z_ref - 1.0),
                      "closure_steps": stats[0], "fallbacks": stats[1]}
     return out
+
+
+def main(argv=None):
+    """The closure experiment at a given scale: filtered-DNS data, GPU training for a time
+    budget, a-posteriori evaluation on a held-out seed (gated and ungated) at 1/4 and all of the
+    run.  Prints one JSON line per evaluation.
+
+        python -m optimizec_b200.closure --nf 2048 --nc 256 --re 1e5 --seeds 8 --steps 67000 \\
+            --every 1000 --train-seconds 420 --batch 4
+    """
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nf", type=int, default=2048)
+    ap.add_argument("--nc", type=int, default=256)
+    ap.add_argument("--re", type=float, default=1e5)
+    ap.add_argument("--seeds", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=67000)
+    ap.add_argument("--every", type=int, default=1000)
+    ap.add_argument("--train-seconds", type=float, default=420.0)
+    ap.add_argument("--batch", type=int, default=4)
+    a = ap.parse_args(argv)
+    cfg = dict(Nf=a.nf, Nc=a.nc, Re=a.re, K0=4.0, cfl=0.1)
+    t = time.time()
+    X, T = generate(seeds=range(a.seeds), steps=a.steps, every=a.every, warm=a.every, **cfg)
+    print(json.dumps({"data": list(X.shape), "generate_s": round(time.time() - t, 1)}), flush=True)
+    t = time.time()
+    net, sc, _ = train(X, T, iters=20, batch=a.batch, lr=1e-3)
+    per = (time.time() - t) / 20
+    iters = max(100, int(a.train_seconds / per))
+    t = time.time()
+    losses = net.train(iters, a.batch, 1e-3, seed=7)
+    print(json.dumps({"train_iters": iters, "train_s": round(time.time() - t, 1),
+                      "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-50:]))}),
+          flush=True)
+    for chk in (1, 0):
+        for fs in (a.steps // 4, a.steps):
+            r = evaluate(net, sc, seed=100, fine_steps=fs, update=100, check=chk, **cfg)
+            r["energy_check"] = chk
+            r["speedup_closure_vs_dns"] = r["wall_dns"] / r["closure"]["wall"]
+            print(json.dumps(r), flush=True)
+    net.close()
+
+
+if __name__ == "__main__":
+    main()
