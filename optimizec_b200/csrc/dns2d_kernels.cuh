@@ -427,30 +427,61 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
             prefetch_l2(o < QB ? b0 + o : b0 + (size_t)L * H * 8 + (o - QB));
     }
 #endif
-    // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW
-    if (j < LR1) {
+    // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW.  Z at
+    // k > L-H needs U, W at L-k = (L/R1 - j) + (R1-1-r) L/R1: slot R1-1-r of butterfly L/R1 - j.
+    // Butterflies j and L/R1 - j share a warp 16 lanes apart, so every thread loads only its
+    // k < H slots and receives the mirrored values from its partner lane; butterflies 0 and
+    // L/R1/2 are their own mirrors (slots R1 - r and R1-1-r of their own loads).  Half the global
+    // loads of reading both mirrors directly (N = 4096 on B200: row pass 0.334 -> 0.309 ms).
+    static_assert(R1 == 16 && LR1 % 32 == 0 && C::NT >= LR1, "mirror pairing");
+    if (j < LR1) {  // whole warps (L/R1 is a multiple of 32)
+        const int lane = j & 31, q = (j >> 5) * 16 + (lane & 15);
+        const int jb = (lane < 16) ? (q == 0 ? 0 : q) : (q == 0 ? LR1 / 2 : LR1 - q);
+        float2 a[R1], b[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            a[r] = make_float2(0.f, 0.f);
+            b[r] = a[r];
+            const int k = jb + r * LR1;
+            if (!slot_in_band<L, R1, H, L - H>(r) && r * LR1 < H && k < H) {
+                a[r] = U[(size_t)k << 2];
+                b[r] = W[(size_t)k << 2];
+            }
+        }
         float2 v[R1];
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
-            if (slot_in_band<L, R1, H, L - H>(r)) {  // inside the zero band for every j
+            const int k = jb + r * LR1;
+            if (slot_in_band<L, R1, H, L - H>(r)) {
                 v[r] = make_float2(0.f, 0.f);
-                continue;
+            } else if ((r + 1) * LR1 <= L - H + 1) {  // slot never above L-H: lo or zero
+                if (k == 0) v[r] = make_float2(a[r].x, b[r].x);
+                else if (k < H) v[r] = make_float2(a[r].x - b[r].y, a[r].y + b[r].x);
+                else v[r] = make_float2(0.f, 0.f);
+            } else {  // slot r can be above L-H: mirrored value from slot R1-1-r of the partner
+                float2 ma, mb;
+                ma.x = __shfl_xor_sync(0xffffffffu, a[R1 - 1 - r].x, 16);
+                ma.y = __shfl_xor_sync(0xffffffffu, a[R1 - 1 - r].y, 16);
+                mb.x = __shfl_xor_sync(0xffffffffu, b[R1 - 1 - r].x, 16);
+                mb.y = __shfl_xor_sync(0xffffffffu, b[R1 - 1 - r].y, 16);
+                if (jb == 0) {
+                    ma = a[(R1 - r) & (R1 - 1)];
+                    mb = b[(R1 - r) & (R1 - 1)];
+                } else if (jb == LR1 / 2) {
+                    ma = a[R1 - 1 - r];
+                    mb = b[R1 - 1 - r];
+                }
+                if (k < H) {
+                    v[r] = (k == 0) ? make_float2(a[r].x, b[r].x) : make_float2(a[r].x - b[r].y, a[r].y + b[r].x);
+                } else if (k > L - H) {
+                    v[r] = make_float2(ma.x + mb.y, mb.x - ma.y);
+                } else {
+                    v[r] = make_float2(0.f, 0.f);
+                }
             }
-            const int k = j + r * LR1;
-            float2 a = make_float2(0.f, 0.f), b = a;
-            const bool lo = k < H, hi = k > L - H;
-            if (lo || hi) {
-                const int kk = lo ? k : L - k;
-                a = U[(size_t)kk << 2];
-                b = W[(size_t)kk << 2];
-            }
-            if (k == 0) v[r] = make_float2(a.x, b.x);
-            else if (lo) v[r] = make_float2(a.x - b.y, a.y + b.x);
-            else if (hi) v[r] = make_float2(a.x + b.y, b.x - a.y);
-            else v[r] = make_float2(0.f, 0.f);
         }
         DFT<R1, true>::run(v);
-        sm_store<L, R1, 1>(s, v, j);
+        sm_store<L, R1, 1>(s, v, jb);
     }
     stage1<TwCat<N>, L, R2, R1, true>(s, p.tw);
     // inverse stage 3 into registers -> products -> forward stage 1
