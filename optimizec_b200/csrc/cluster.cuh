@@ -138,8 +138,30 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, 1) k_ro
     const Peers pe(cl, s);
     const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
     const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
-    for (int k2 = threadIdx.x; k2 < M; k2 += NT) s[sidx(k2)] = packed_uw<L, H>(U, W, 4 * k2 + c);
-    __syncthreads();
+    // Q[k] of the Hermitian packing belongs to CTA k % 4 at position k / 4.  Each CTA reads a
+    // contiguous quarter of U, W (k < H) once and stores Q[k] and Q[L-k] into the owners' shared
+    // memory; the zero band [H, L-H] is cleared locally.  The first barrier makes sure every CTA
+    // of the cluster runs before shared memory is written across it.
+    for (int k2 = threadIdx.x; k2 < M; k2 += NT) {
+        const int k = 4 * k2 + c;
+        if (k >= H && k <= L - H) s[sidx(k2)] = make_float2(0.f, 0.f);
+    }
+    cl.sync();
+    {
+        constexpr int HQ = (H + 3) / 4;
+        const int k0 = c * HQ, k1 = min(H, k0 + HQ);
+        for (int k = k0 + (int)threadIdx.x; k < k1; k += NT) {
+            const float2 a = U[(size_t)k << 2], b = W[(size_t)k << 2];
+            if (k == 0) {
+                pe.p[0][sidx(0)] = make_float2(a.x, b.x);
+            } else {
+                pe.p[k & 3][sidx(k >> 2)] = make_float2(a.x - b.y, a.y + b.x);
+                const int km = L - k;
+                pe.p[km & 3][sidx(km >> 2)] = make_float2(a.x + b.y, b.x - a.y);
+            }
+        }
+    }
+    cl.sync();
     fft_run<Cat, M, MP, true, 1, NT>(s, p.tw, typename C::Plan{});
     cl.sync();
     const int m1 = min(M, (c + 1) * MQ);
@@ -153,17 +175,20 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, 1) k_ro
     cl.sync();
     fft_run<Cat, M, MP, false, 1, NT>(s, p.tw, typename C::Plan{});
     cl.sync();
-    // unpack D = (Q[k] + conj Q[L-k]) / 2, E = -i (Q[k] - conj Q[L-k]) / 4 for k = 4 k2 + c < H;
-    // Q[L-k] sits in CTA (L-k) % 4 at position (L-k) / 4
+    // unpack D = (Q[k] + conj Q[L-k]) / 2, E = -i (Q[k] - conj Q[L-k]) / 4 for k < H; Q[k] sits in
+    // CTA k % 4 at position k / 4.  Each CTA writes a contiguous quarter of the k range.
     float2 *__restrict__ Do = p.work + widx<L, H>(0, z, 0);
     float2 *__restrict__ Eo = p.work + widx<L, H>(1, z, 0);
-    for (int k2 = threadIdx.x; 4 * k2 + c < H; k2 += NT) {
-        const int k = 4 * k2 + c;
-        const int kp = (k == 0) ? 0 : L - k;
-        const float2 q = s[sidx(k2)];
-        const float2 m = pe.p[kp & 3][sidx(kp >> 2)];
-        Do[(size_t)k << 2] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
-        Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
+    {
+        constexpr int HQ = (H + 3) / 4;
+        const int k0 = c * HQ, k1 = min(H, k0 + HQ);
+        for (int k = k0 + (int)threadIdx.x; k < k1; k += NT) {
+            const int kp = (k == 0) ? 0 : L - k;
+            const float2 q = pe.p[k & 3][sidx(k >> 2)];
+            const float2 m = pe.p[kp & 3][sidx(kp >> 2)];
+            Do[(size_t)k << 2] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
+            Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
+        }
     }
     cl.sync();
 }
