@@ -151,6 +151,10 @@ void dns2d_batch_destroy(dns2d_batch *b);
 const char *dns2d_batch_last_error(const dns2d_batch *b);
 void *dns2d_batch_stream(dns2d_batch *b);
 /* every member from its own seeded k^4 field (then call dns2d_batch_next_dt) */
+/* Autotuner for a batch (no counterpart in the reference): times each size group's kernel
+ * variants at the group's member count on the batch's buffers and keeps the fastest; call before
+ * dns2d_batch_init_k4 (DNS2D_ERR_STATE after it).  Variants compute the same arithmetic. */
+int dns2d_batch_autotune(dns2d_batch *b);
 int dns2d_batch_init_k4(dns2d_batch *b);
 /* NEXTDT for every member; cflm (nullable) receives count values */
 int dns2d_batch_next_dt(dns2d_batch *b, float *cflm);
@@ -205,6 +209,18 @@ int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
 /* 1 (default): the closure network runs on the BF16 tensor-core path where the grid allows it
  * (L % 128 == 0, 32 channels); 0: FP32 on the SIMT pipes everywhere. */
 int dns2d_closure_tensor_cores(dns2d_state *s, int enable);
+
+/* Autotuner (no counterpart in the reference): times the kernel variants of size N on a scratch
+ * state on `device` -- rows per CTA of the small-grid row pass, one or two thread groups per
+ * column CTA and the L2 prefetch distances of the large-grid passes -- and keeps the fastest for
+ * states and batches created afterwards on that device.  All variants compute the same
+ * arithmetic, so results do not depend on the choice.  config (nullable) receives
+ * {rows_tile, cols_groups, pf_rows, pf_cols} (0 = the size's default).  DNS2D_AUTOTUNE=1 in the
+ * environment makes dns2d_create tune its size once per process. */
+int dns2d_autotune(int N, int device, int *config);
+/* Pin a configuration {rows_tile (0, 2, 4, 8), cols_groups (0, 1, 2), pf_rows, pf_cols} for size
+ * N on `device` (no counterpart in the reference); used by states created afterwards. */
+int dns2d_set_tuning(int N, int device, const int *config);
 
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */
 int dns2d_phase_timing(dns2d_state *s, int enable);

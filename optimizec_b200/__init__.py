@@ -42,7 +42,7 @@ SYMBOLS = [
     "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
-    "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores",
+    "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -159,6 +159,9 @@ def lib():
         "dns2d_closure_forcing": (C.c_int, [vp, fp]),
         "dns2d_cnn_forward_tc": (C.c_int, [vp, fp, C.c_int, C.c_int, C.c_int, fp]),
         "dns2d_closure_tensor_cores": (C.c_int, [vp, C.c_int]),
+        "dns2d_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
+        "dns2d_set_tuning": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
+        "dns2d_batch_autotune": (C.c_int, [vp]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
@@ -179,6 +182,23 @@ def _dp(a):
 
 def supported(N: int) -> bool:
     return bool(lib().dns2d_supported(N))
+
+
+def autotune(N: int, device: int = 0) -> dict:
+    """Time the kernel variants of size N and keep the fastest (dns2d_autotune)."""
+    cfg = (C.c_int * 4)()
+    rc = lib().dns2d_autotune(N, device, cfg)
+    if rc:
+        raise Dns2dError(f"dns2d_autotune: {lib().dns2d_strerror(rc).decode()}")
+    return dict(zip(("rows_tile", "cols_groups", "pf_rows", "pf_cols"), list(cfg)))
+
+
+def set_tuning(N: int, rows_tile=0, cols_groups=0, pf_rows=296, pf_cols=74, device: int = 0):
+    """Pin the kernel configuration of size N (dns2d_set_tuning)."""
+    cfg = (C.c_int * 4)(rows_tile, cols_groups, pf_rows, pf_cols)
+    rc = lib().dns2d_set_tuning(N, device, cfg)
+    if rc:
+        raise Dns2dError(f"dns2d_set_tuning: {lib().dns2d_strerror(rc).decode()}")
 
 
 def k4_spectrum(N: int, K0: float, seed: int) -> np.ndarray:
@@ -398,6 +418,10 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+    def autotune(self):
+        """Time each size group's kernel variants at its member count (before init_k4)."""
+        self._chk(self._L.dns2d_batch_autotune(self._b))
 
     def init_k4(self):
         self._chk(self._L.dns2d_batch_init_k4(self._b))

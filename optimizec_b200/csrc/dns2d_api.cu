@@ -19,6 +19,7 @@
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -69,7 +70,14 @@ struct Launch {
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
         }
-        if ((e = cudaFuncSetAttribute(k_rows_step<N>, a, (int)smB)) != cudaSuccess) return e;
+        if constexpr (!V2) {  // the rows-per-CTA variants of the small-grid row pass
+            if ((e = cudaFuncSetAttribute(k_rows_step<N, 2>, a, (int)(2 * C::LP * sizeof(float2)))) != cudaSuccess)
+                return e;
+            if ((e = cudaFuncSetAttribute(k_rows_step<N, 4>, a, (int)(4 * C::LP * sizeof(float2)))) != cudaSuccess)
+                return e;
+            if ((e = cudaFuncSetAttribute(k_rows_step<N, 8>, a, (int)(8 * C::LP * sizeof(float2)))) != cudaSuccess)
+                return e;
+        }
         if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_init<N>, a, (int)smA)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_rows_velocity<N>, a, (int)smB)) != cudaSuccess) return e;
@@ -82,16 +90,26 @@ struct Launch {
     }
     static void rows_step(const Pointers &p, cudaStream_t s, int ny)
     {
-        if constexpr (V2) k_rows_step2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p);
-        else k_rows_step<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p);
+        if constexpr (V2) {
+            k_rows_step2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p);
+        } else {
+            // rows per CTA (autotuned): 2, 4 or 8; the arithmetic per row is the same
+            const int rt = p.rows_tile ? p.rows_tile : C::ROWS;
+            const size_t sm = (size_t)rt * C::LP * sizeof(float2);
+            if (rt == 2) k_rows_step<N, 2><<<dim3(C::L / 2, ny), C::NTB, sm, s>>>(p);
+            else if (rt == 8) k_rows_step<N, 8><<<dim3(C::L / 8, ny), C::NTB, sm, s>>>(p);
+            else k_rows_step<N, 4><<<dim3(C::L / 4, ny), C::NTB, sm, s>>>(p);
+        }
     }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
     {
-        // two thread groups per column CTA pay off once a column is long enough (measured on
-        // B200: faster at N = 4096, slower at 2048)
-        if constexpr (V2 && N >= 4096)
-            k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
-        else if constexpr (V2) k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        // two thread groups per column CTA (autotuned; default from B200 measurements: faster at
+        // N = 4096, slower at 2048); both give the same arithmetic
+        if constexpr (V2) {
+            const int g = p.cols_groups ? p.cols_groups : (N >= 4096 ? 2 : 1);
+            if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+            else k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+        }
         else k_cols_step<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
     }
     static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
@@ -185,6 +203,31 @@ struct LaunchC {
                          rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr};
     }
 };
+
+// kernel configuration of one size on one device; every variant computes the same arithmetic,
+// so the choice changes speed only
+struct Tuning {
+    int rows_tile = 0, cols_groups = 0, pf_rows = 296, pf_cols = 74;
+};
+
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, Tuning> g_tune;  // (device, N) -> autotuned configuration
+thread_local bool t_in_autotune = false;       // the autotuner's own scratch state is untuned
+
+Tuning tuning_for(int device, int N)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({device, N});
+    return it == g_tune.end() ? Tuning() : it->second;
+}
+
+void apply_tuning(Pointers &p, const Tuning &t)
+{
+    p.rows_tile = t.rows_tile;
+    p.cols_groups = t.cols_groups;
+    p.pf_rows = t.pf_rows;
+    p.pf_cols = t.pf_cols;
+}
 
 const KernelSet *kernel_set(int N)
 {
@@ -420,6 +463,7 @@ struct dns2d_state {
     float in_scale[3] = {1, 1, 1}, out_scale = 1;
     int closure_check = 1;
     int closure_tc = 1;  // BF16 tensor-core CNN inference where the grid allows it
+    Tuning tune;         // kernel configuration (from the autotuner's table at creation)
     float2 *force = nullptr, *bk_om2 = nullptr, *bk_fnm1 = nullptr, *bk_work = nullptr;
     float *gate = nullptr;                  // device 0/1 per step (energy gate)
     double2 *gate_part = nullptr;           // per-block partials of the gate reduction
@@ -448,6 +492,7 @@ struct dns2d_state {
         p.s_work = 0;
         p.s_part = 0;
         p.s_hist = 0;
+        apply_tuning(p, tune);
         return p;
     }
 };
@@ -566,6 +611,18 @@ extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float 
     *out = nullptr;
     const KernelSet *ks = kernel_set(N);
     if (!ks) return DNS2D_ERR_SIZE;
+    if (!t_in_autotune) {
+        const char *env = std::getenv("DNS2D_AUTOTUNE");
+        bool tuned;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            tuned = g_tune.count({device, N}) > 0;
+        }
+        if (env && env[0] == '1' && !tuned) {
+            const int rc = dns2d_autotune(N, device, nullptr);
+            if (rc) return rc;
+        }
+    }
     dns2d_state *s = new dns2d_state();
     s->N = N;
     s->H = N / 2;
@@ -577,6 +634,7 @@ extern "C" int dns2d_create(dns2d_state **out, int N, float Re, float K0, float 
     s->cflnum = cflnum;
     s->device = device;
     s->ks = ks;
+    s->tune = tuning_for(device, N);
     auto bail = [&](int rc) {
         dns2d_destroy(s);
         return rc;
@@ -1546,6 +1604,7 @@ struct BatchGroup {
     double2 *part = nullptr, *hist = nullptr;
     unsigned int *counter = nullptr;
     float *cflm = nullptr;
+    Tuning tune;
 
     Pointers ptrs() const
     {
@@ -1564,6 +1623,7 @@ struct BatchGroup {
         p.s_work = 2 * (size_t)L * H;
         p.s_part = H;
         p.s_hist = kChunk;
+        apply_tuning(p, tune);
         return p;
     }
 };
@@ -1669,6 +1729,7 @@ extern "C" int dns2d_batch_create(dns2d_batch **out, const dns2d_member *members
             g.H = m.N / 2;
             g.L = 3 * m.N / 2;
             g.ks = kernel_set(m.N);
+            g.tune = tuning_for(device, m.N);
             b->groups.push_back(g);
             gi = (int)b->groups.size() - 1;
         }
@@ -1736,6 +1797,77 @@ static int batch_velocity(dns2d_batch *b)
     BATCH_CUDA(cudaStreamSynchronize(b->stream), "batch velocity");
     b->initialised = true;
     return DNS2D_OK;
+}
+
+// Autotuner for a batch: each size group's kernel variants timed with the group's own member
+// count on the batch's own buffers.  Call before the initial fields are set (the timing runs
+// the passes on the buffers); every variant computes the same arithmetic.
+extern "C" int dns2d_batch_autotune(dns2d_batch *b)
+{
+    if (!b) return DNS2D_ERR_ARG;
+    if (b->initialised) return DNS2D_ERR_STATE;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return DNS2D_ERR_CUDA;
+    }
+    auto timed = [&](auto fn, int reps) {
+        for (int i = 0; i < 2; ++i) fn();
+        cudaEventRecord(e0, b->stream);
+        for (int i = 0; i < reps; ++i) fn();
+        cudaEventRecord(e1, b->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / (float)reps;
+    };
+    for (BatchGroup &g : b->groups) {
+        if (g.N == 840 || g.N == 29400) continue;
+        const int reps = g.N >= 2048 ? 10 : 50;
+        Tuning best = g.tune;
+        float tb = 1e30f;
+        if (g.N >= 1024) {
+            for (int pf : {0, 148, 296, 592}) {
+                g.tune = best;
+                g.tune.pf_rows = pf;
+                const Pointers p = g.ptrs();
+                const float t = timed([&] { g.ks->rows_step(p, b->stream, g.count); }, reps);
+                if (t < tb) tb = t, best.pf_rows = pf;
+            }
+            tb = 1e30f;
+            for (int gr : {1, 2})
+                for (int pf : {0, 37, 74, 148}) {
+                    g.tune = best;
+                    g.tune.cols_groups = gr;
+                    g.tune.pf_cols = pf;
+                    const Pointers p = g.ptrs();
+                    const float t = timed([&] { g.ks->cols_step(p, 0, 0, b->stream, g.count); }, reps);
+                    if (t < tb) tb = t, best.cols_groups = gr, best.pf_cols = pf;
+                }
+        } else {
+            for (int rt : {2, 4, 8}) {
+                g.tune = best;
+                g.tune.rows_tile = rt;
+                const Pointers p = g.ptrs();
+                const float t = timed([&] { g.ks->rows_step(p, b->stream, g.count); }, reps);
+                if (t < tb) tb = t, best.rows_tile = rt;
+            }
+        }
+        g.tune = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the buffers hold timing leftovers: clear them as at creation
+    for (BatchGroup &g : b->groups) {
+        const size_t nom = (size_t)g.count * g.N * g.H, nwork = (size_t)g.count * 2 * g.L * g.H;
+        if (cudaMemsetAsync(g.om2, 0, nom * 8, b->stream) != cudaSuccess ||
+            cudaMemsetAsync(g.fnm1, 0, nom * 8, b->stream) != cudaSuccess ||
+            cudaMemsetAsync(g.work, 0, nwork * 8, b->stream) != cudaSuccess)
+            return DNS2D_ERR_CUDA;
+    }
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    return cudaStreamSynchronize(b->stream) == cudaSuccess ? DNS2D_OK : DNS2D_ERR_CUDA;
 }
 
 extern "C" int dns2d_batch_init_k4(dns2d_batch *b)
@@ -1918,6 +2050,110 @@ extern "C" int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars
 // ============================================================================================
 // Learned-closure network (cnn.cuh): parameters, activations, dataset and Adam state on the
 // device; forward / backward / training driven from here.
+// ============================================================================================
+// Autotuner: times the kernel variants of one size on a scratch state (k^4 field) and keeps
+// the fastest per (device, N).  The variants differ in rows per CTA (small grids), thread groups
+// per column CTA and L2 prefetch distances (large grids) and compute the same arithmetic, so a
+// tuned run gives the same results as an untuned one.  States and batches created afterwards on
+// that device use the choice; DNS2D_AUTOTUNE=1 in the environment tunes at dns2d_create.
+// ============================================================================================
+namespace {
+// mean ms of one launch of fn over reps launches (after 2 warm-up launches) on the state's stream
+template <class F>
+float time_launches(dns2d_state *s, int reps, F fn)
+{
+    for (int i = 0; i < 2; ++i) fn();
+    cudaEventRecord(s->ev0, s->stream);
+    for (int i = 0; i < reps; ++i) fn();
+    cudaEventRecord(s->ev1, s->stream);
+    cudaEventSynchronize(s->ev1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    return ms / (float)reps;
+}
+}  // namespace
+
+extern "C" int dns2d_set_tuning(int N, int device, const int *config)
+{
+    if (!kernel_set(N) || !config) return DNS2D_ERR_ARG;
+    if (!(config[0] == 0 || config[0] == 2 || config[0] == 4 || config[0] == 8) || config[1] < 0 || config[1] > 2 ||
+        config[2] < 0 || config[3] < 0)
+        return DNS2D_ERR_ARG;
+    Tuning t;
+    t.rows_tile = config[0];
+    t.cols_groups = config[1];
+    t.pf_rows = config[2];
+    t.pf_cols = config[3];
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{device, N}] = t;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_autotune(int N, int device, int *config)
+{
+    const KernelSet *ks = kernel_set(N);
+    if (!ks) return DNS2D_ERR_SIZE;
+    Tuning best;
+    if (N != 840 && N != 29400) {  // the cluster sizes have a single configuration
+        t_in_autotune = true;
+        dns2d_state *s = nullptr;
+        int rc = dns2d_create(&s, N, 1.0e5f, 4.0f, 0.1f, device);
+        if (!rc) rc = dns2d_init_k4(s, 1);
+        if (!rc) rc = dns2d_next_dt(s, nullptr);
+        if (!rc) rc = dns2d_step(s, 1, nullptr, nullptr);
+        if (!rc) rc = dns2d_sync(s, 0);
+        t_in_autotune = false;
+        if (rc) {
+            dns2d_destroy(s);
+            return rc;
+        }
+        const int reps = N >= 2048 ? 20 : 100;
+        const bool large = N >= 1024;
+        float tb = 1e30f;
+        if (large) {
+            for (int pf : {0, 148, 296, 592}) {
+                s->tune = best;
+                s->tune.pf_rows = pf;
+                const Pointers p = s->ptrs();
+                const float t = time_launches(s, reps, [&] { ks->rows_step(p, s->stream, 1); });
+                if (t < tb) tb = t, best.pf_rows = pf;
+            }
+            tb = 1e30f;
+            for (int g : {1, 2})
+                for (int pf : {0, 37, 74, 148}) {
+                    s->tune = best;
+                    s->tune.cols_groups = g;
+                    s->tune.pf_cols = pf;
+                    const Pointers p = s->ptrs();
+                    const float t = time_launches(s, reps, [&] { ks->cols_step(p, 0, 0, s->stream, 1); });
+                    if (t < tb) tb = t, best.cols_groups = g, best.pf_cols = pf;
+                }
+        } else {
+            for (int rt : {2, 4, 8}) {
+                s->tune = best;
+                s->tune.rows_tile = rt;
+                const Pointers p = s->ptrs();
+                const float t = time_launches(s, reps, [&] { ks->rows_step(p, s->stream, 1); });
+                if (t < tb) tb = t, best.rows_tile = rt;
+            }
+        }
+        const cudaError_t e = cudaStreamSynchronize(s->stream);
+        dns2d_destroy(s);
+        if (e != cudaSuccess) return DNS2D_ERR_CUDA;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[{device, N}] = best;
+    }
+    if (config) {
+        config[0] = best.rows_tile;
+        config[1] = best.cols_groups;
+        config[2] = best.pf_rows;
+        config[3] = best.pf_cols;
+    }
+    return DNS2D_OK;
+}
+
 // ============================================================================================
 struct dns2d_cnn {
     int layers = 0, channels = 0, device = 0, nparams = 0;

@@ -24,16 +24,6 @@
 #pragma once
 #include "fft.cuh"
 
-// L2 prefetch distances of the large-grid passes, in CTAs ahead of the current one (0 = off).
-// A row CTA brings to L2 the input of the row two waves of resident CTAs later (148 SMs x 2
-// CTAs); a column CTA the input of the column half a wave later.  Measured on B200 at N = 4096:
-// rows 0.348 -> 0.341 ms.
-#ifndef DNS2D_PF_ROWS
-#define DNS2D_PF_ROWS 296
-#endif
-#ifndef DNS2D_PF_COLS
-#define DNS2D_PF_COLS 74
-#endif
 
 namespace dns2d {
 
@@ -103,6 +93,11 @@ struct Pointers {
     // partials, counter and history at these strides (all 0 for a single run)
     size_t s_state, s_work;
     int s_part, s_hist;
+    // kernel configuration (the autotuner's choice; every choice gives the same arithmetic):
+    // rows per CTA of the small-grid row pass (0: the size's default), thread groups per column
+    // CTA of the large-grid column pass (0: default), L2 prefetch distances in CTAs (0: off)
+    int rows_tile = 0, cols_groups = 0;
+    int pf_rows = 296, pf_cols = 74;
 
     __device__ __forceinline__ Pointers member(int m) const
     {
@@ -199,12 +194,12 @@ __device__ __forceinline__ void rows_load_pack(float2 *s, const float2 *__restri
 // ------------------------------------------------------------------------------------------
 // Row pass of one step.
 // ------------------------------------------------------------------------------------------
-template <int N>
+template <int N, int ROWS = Cfg<N>::ROWS>
 __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p0)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
-    constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTB;
     extern __shared__ float2 smem[];
     const int z0 = blockIdx.x * ROWS;
     rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
@@ -417,16 +412,15 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
     const int j = threadIdx.x;
     const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
     const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
-#if DNS2D_PF_ROWS
-    // bring to L2 the quarter (z % 4) of the 4-row tile that the CTA about one wave later reads
-    if (z + DNS2D_PF_ROWS < L) {
-        const int t = (z + DNS2D_PF_ROWS) >> 2, part = z & 3;
+    // bring to L2 the quarter (z % 4) of the 4-row tile that the CTA pf_rows later reads (two
+    // waves of 148 SMs x 2 CTAs by default)
+    if (p.pf_rows > 0 && z + p.pf_rows < L) {
+        const int t = (z + p.pf_rows) >> 2, part = z & 3;
         constexpr int QB = H * 32 / 4;  // bytes of one quarter tile of one component
         const char *b0 = reinterpret_cast<const char *>(p.work + (size_t)t * H * 4) + part * QB;
         for (int o = j * 128; o < 2 * QB; o += C::NT * 128)
             prefetch_l2(o < QB ? b0 + o : b0 + (size_t)L * H * 8 + (o - QB));
     }
-#endif
     // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW.  Z at
     // k > L-H needs U, W at L-k = (L/R1 - j) + (R1-1-r) L/R1: slot R1-1-r of butterfly L/R1 - j.
     // Butterflies j and L/R1 - j share a warp 16 lanes apart, so every thread loads only its
@@ -734,15 +728,13 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, 1) k_cols_step4(Pointers p0, 
         prefetch_l2(om2c + o);
         prefetch_l2(fnc + o);
     }
-#if DNS2D_PF_COLS
-    if (kx + DNS2D_PF_COLS < (int)gridDim.x) {
-        const int kp = kx + DNS2D_PF_COLS;
+    if (p.pf_cols > 0 && kx + p.pf_cols < (int)gridDim.x) {  // the column pf_cols CTAs later
+        const int kp = kx + p.pf_cols;
         for (int q = (int)threadIdx.x; q < 2 * (L / 4); q += NT2) {
             const int a = q / (L / 4), gg = q - a * (L / 4);
             prefetch_l2(p.work + (size_t)a * L * H + (((size_t)gg * H + kp) << 2));
         }
     }
-#endif
     cp_async_wait<0>();
     stage1g<TwCat<N>, L, R3, 1, false, NT>(sg, p.tw, j, bar);
     stage1g<TwCat<N>, L, R2, R3, false, NT>(sg, p.tw, j, bar);

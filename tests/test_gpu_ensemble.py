@@ -51,3 +51,24 @@ def test_ensemble_configuration():
     # viscous decay of the high-Re members (~1e-8) is below FP32 rounding of the nonlinear term
     assert np.all(E[:, -1] < E[:, 0])
     b.close()
+
+
+def test_batch_autotune_keeps_results():
+    """dns2d_batch_autotune (before init) picks kernel variants with the same arithmetic: the
+    tuned batch reproduces the untuned one bit for bit."""
+    import optimizec_b200 as P
+    ms = [(128, 3e3, 3.0, 0.1, 1), (256, 1e4, 4.0, 0.1, 2), (128, 1e4, 5.0, 0.1, 3), (1024, 1e4, 4.0, 0.1, 4)]
+    out = []
+    for tune in (False, True):
+        b = P.Batch(ms)
+        if tune:
+            b.autotune()
+        b.init_k4()
+        b.next_dt()
+        b.step(1)
+        b.next_dt()
+        b.step(9)
+        out.append([b.om2(m) for m in range(len(ms))])
+        b.close()
+    for a, c in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, c)
