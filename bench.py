@@ -83,6 +83,22 @@ def parse():
     return a
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The maximum of a per-rank value over all ranks (the slowest replica's time)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps: int, ms_max: float, world: int) -> float:
+    """Whole-job steps/s of `world` independent replicas that each ran `steps` steps, timed by
+    the slowest one."""
+    return world * steps / (ms_max / 1e3)
+
+
 def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -206,12 +222,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ck = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+    ms_max = max_over_ranks(ms, world, device=f"cuda:{local_rank}")
     if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
-    ms_max = float(t.item())
-    value = world * K / (ms_max / 1e3)
+    value = replica_throughput(K, ms_max, world)
 
     # per-kernel device time (CUDA events around each launch, on the solver's stream)
     s.phase_timing(True)
@@ -257,11 +271,7 @@ def run_e2e(s_old, P, N, K, W, up, local_rank, world):
     res_fn = s.fnm1()
     out_om[...] = res_om.view(np.float32).reshape(N, H, 2)
     t1 = time.perf_counter()
-    sec = t1 - t0
-    t = torch.tensor([sec], device=f"cuda:{local_rank}", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    sec = float(t.item())
+    sec = max_over_ranks(t1 - t0, world, device=f"cuda:{local_rank}")
     s.close()
     state_bytes = 2 * N * H * 8
     return {"value": world * K / sec, "unit": "steps/s",

@@ -205,6 +205,8 @@ int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int
  * layout of dns2d_get_fnm1 (N x N/2 complex float, [kz][kx]); a diagnostic, the state is not
  * advanced. */
 int dns2d_closure_forcing(dns2d_state *s, float *force);
+/* Closed steps and fallbacks so far; DNS2D_ERR_TIMEOUT if a tensor-core wait of the closure
+ * network ran out (its bounded mbarrier wait sets a device flag instead of hanging). */
 int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
 /* 1 (default): the closure network runs on the BF16 tensor-core path where the grid allows it
  * (L % 128 == 0, 32 channels); 0: FP32 on the SIMT pipes everywhere. */

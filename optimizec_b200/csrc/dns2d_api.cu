@@ -2902,6 +2902,12 @@ extern "C" int dns2d_closure_forcing(dns2d_state *s, float *force)
 extern "C" int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks)
 {
     if (!s) return DNS2D_ERR_ARG;
+    if (s->cnn && s->cnn->tc_err) {  // a tensor-core wait that ran out marks the closure unusable
+        int flag = 0;
+        DNS2D_CUDA(cudaMemcpyAsync(&flag, s->cnn->tc_err, 4, cudaMemcpyDeviceToHost, s->stream), "flag copy");
+        DNS2D_CUDA(cudaStreamSynchronize(s->stream), "flag sync");
+        if (flag) return fail(s, DNS2D_ERR_TIMEOUT, "tensor-core MMA completion wait timed out in the closure network");
+    }
     if (steps) *steps = s->closure_steps;
     if (fallbacks) {
         unsigned long long gated = 0;
