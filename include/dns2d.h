@@ -211,6 +211,10 @@ int dns2d_closure_stats(dns2d_state *s, long long *steps, long long *fallbacks);
 /* 1 (default): the closure network runs on the BF16 tensor-core path where the grid allows it
  * (L % 128 == 0, 32 channels); 0: FP32 on the SIMT pipes everywhere. */
 int dns2d_closure_tensor_cores(dns2d_state *s, int enable);
+/* Forcing limiter (default off): each mode's closure forcing is limited in magnitude to alpha
+ * times the resolved nonlinear term FN of the same mode, so the closure cannot act where the
+ * resolved transfer vanishes (e.g. shells the cascade has not reached yet). */
+int dns2d_closure_clamp(dns2d_state *s, float alpha);
 
 /* Autotuner (no counterpart in the reference): times the kernel variants of size N on a scratch
  * state on `device` -- rows per CTA of the small-grid row pass, one or two thread groups per

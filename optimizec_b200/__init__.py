@@ -42,7 +42,7 @@ SYMBOLS = [
     "dns2d_cnn_create", "dns2d_cnn_destroy", "dns2d_cnn_last_error", "dns2d_cnn_num_params",
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
-    "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune",
+    "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -162,6 +162,7 @@ def lib():
         "dns2d_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
         "dns2d_set_tuning": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
         "dns2d_batch_autotune": (C.c_int, [vp]),
+        "dns2d_closure_clamp": (C.c_int, [vp, C.c_float]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
@@ -372,6 +373,10 @@ class Solver:
         out = np.zeros((self.N, self.H), dtype=np.complex64)
         self._chk(self._L.dns2d_closure_forcing(self._s, _fp(out.view(np.float32))))
         return out
+
+    def closure_clamp(self, alpha: float):
+        """Limit each mode's closure forcing to alpha |FN| (0: off)."""
+        self._chk(self._L.dns2d_closure_clamp(self._s, float(alpha)))
 
     def closure_tensor_cores(self, enable: bool):
         self._chk(self._L.dns2d_closure_tensor_cores(self._s, int(enable)))

@@ -111,7 +111,8 @@ def shells(om: np.ndarray) -> np.ndarray:
     return np.bincount(sh.ravel(), weights=e.ravel(), minlength=N)
 
 
-def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine_steps=2000, update=100, check=1):
+def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine_steps=2000, update=100, check=1,
+             clamp=0.0):
     """Filtered DNS vs coarse runs with and without the closure over the same physical time."""
     f = Solver(Nf, Re, K0, cfl)
     f.init_k4(seed)
@@ -137,6 +138,8 @@ def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine
         c.next_dt()
         if with_closure:
             c.attach_closure(net, scales, energy_check=check)
+            if clamp > 0.0:
+                c.closure_clamp(clamp)
         # same diagnostic cadence as the DNS; stop at the step closest to the DNS end time
         t0 = time.perf_counter()
         n = 0
@@ -158,7 +161,7 @@ def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine
         c.close()
         return om, wall, n, tc, stats
 
-    out = {"t_end": t_end, "wall_dns": wall_f, "fine_steps": fine_steps}
+    out = {"t_end": t_end, "wall_dns": wall_f, "fine_steps": fine_steps, "clamp": clamp}
     E_ref = shells(ref)
     Z_ref = float(np.sum(np.abs(ref.astype(np.complex128)) ** 2 * np.where(np.arange(Nc // 2) == 0, 0.5, 1.0)))
     kmax = Nc // 2 - 1
@@ -175,8 +178,8 @@ def evaluate(net, scales, Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seed=100, fine
 
 def main(argv=None):
     """The closure experiment at a given scale: filtered-DNS data, GPU training for a time
-    budget, a-posteriori evaluation on a held-out seed (gated and ungated) at 1/4 and all of the
-    run.  Prints one JSON line per evaluation.
+    budget, a-posteriori evaluation on a held-out seed (energy gate with and without the forcing
+    limiter, and ungated) at 1/4 and all of the run.  Prints one JSON line per evaluation.
 
         python -m optimizec_b200.closure --nf 2048 --nc 256 --re 1e5 --seeds 8 --steps 67000 \\
             --every 1000 --train-seconds 420 --batch 4
@@ -193,6 +196,7 @@ def main(argv=None):
     ap.add_argument("--every", type=int, default=1000)
     ap.add_argument("--train-seconds", type=float, default=420.0)
     ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--clamp", type=float, default=1.0, help="forcing limiter alpha (0: off)")
     a = ap.parse_args(argv)
     cfg = dict(Nf=a.nf, Nc=a.nc, Re=a.re, K0=4.0, cfl=0.1)
     t = time.time()
@@ -207,9 +211,9 @@ def main(argv=None):
     print(json.dumps({"train_iters": iters, "train_s": round(time.time() - t, 1),
                       "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-50:]))}),
           flush=True)
-    for chk in (1, 0):
+    for chk, clamp in ((1, a.clamp), (1, 0.0), (0, 0.0)):
         for fs in (a.steps // 4, a.steps):
-            r = evaluate(net, sc, seed=100, fine_steps=fs, update=100, check=chk, **cfg)
+            r = evaluate(net, sc, seed=100, fine_steps=fs, update=100, check=chk, clamp=clamp, **cfg)
             r["energy_check"] = chk
             r["speedup_closure_vs_dns"] = r["wall_dns"] / r["closure"]["wall"]
             print(json.dumps(r), flush=True)

@@ -310,12 +310,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, 1)
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
-            if (p.force) {
-                const float g = p.gate ? *p.gate : 1.0f;
-                const float2 f = p.force[(size_t)kx * N + iz];
-                fn.x += g * f.x;
-                fn.y += g * f.y;
-            }
+            if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;

@@ -463,6 +463,7 @@ struct dns2d_state {
     float in_scale[3] = {1, 1, 1}, out_scale = 1;
     int closure_check = 1;
     int closure_tc = 1;  // BF16 tensor-core CNN inference where the grid allows it
+    float closure_clamp = 0.0f;  // forcing limited to this multiple of |FN| per mode (0: off)
     Tuning tune;         // kernel configuration (from the autotuner's table at creation)
     float2 *force = nullptr, *bk_om2 = nullptr, *bk_fnm1 = nullptr, *bk_work = nullptr;
     float *gate = nullptr;                  // device 0/1 per step (energy gate)
@@ -2711,6 +2712,7 @@ static int closure_device_step(dns2d_state *s, int first, int slot)
     if (rc) return rc;
     Pointers p = s->ptrs();
     p.force = s->force;
+    p.force_clamp = s->closure_clamp;
     if (s->closure_check == 1) {
         k_closure_gate<<<kGateBlocks, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off,
                                                           s->gate_part, s->gate_counter);
@@ -2794,6 +2796,7 @@ static int closure_run(dns2d_state *s, int nsteps, double *E_hist, double *Z_his
         if (rc) return rc;
         Pointers p = s->ptrs();
         p.force = s->force;
+        p.force_clamp = s->closure_clamp;
         s->ks->rows_step(p, s->stream, 1);
         s->ks->cols_step(p, 1, 0, s->stream, 1);
         DNS2D_LAUNCHED("closure step");
@@ -2878,6 +2881,16 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
 
 // forcing spectrum that the attached closure adds to FN for the current state (compact layout of
 // dns2d_get_fnm1)
+// forcing limiter of the attached closure: per mode |forcing| <= alpha |FN| (alpha <= 0: off)
+extern "C" int dns2d_closure_clamp(dns2d_state *s, float alpha)
+{
+    if (!s) return DNS2D_ERR_ARG;
+    s->closure_clamp = alpha > 0.0f ? alpha : 0.0f;
+    for (auto &kv : s->closure_graphs) cudaGraphExecDestroy(kv.second);
+    s->closure_graphs.clear();
+    return DNS2D_OK;
+}
+
 // BF16 tensor-core inference of the attached closure network (default on where the grid allows
 // it); 0 runs the FP32 SIMT network
 extern "C" int dns2d_closure_tensor_cores(dns2d_state *s, int enable)

@@ -98,6 +98,8 @@ struct Pointers {
     // CTA of the large-grid column pass (0: default), L2 prefetch distances in CTAs (0: off)
     int rows_tile = 0, cols_groups = 0;
     int pf_rows = 296, pf_cols = 74;
+    // closure forcing limiter: |forcing| <= force_clamp |FN| per mode (0: off)
+    float force_clamp = 0.0f;
 
     __device__ __forceinline__ Pointers member(int m) const
     {
@@ -118,6 +120,24 @@ struct Pointers {
 // ------------------------------------------------------------------------------------------
 // helpers
 // ------------------------------------------------------------------------------------------
+
+// FN of mode (kx, iz) plus the closure forcing: times the energy gate (0/1), and with a clamp
+// alpha > 0 limited in magnitude to alpha |FN| of the same mode (where the resolved transfer
+// vanishes, e.g. shells the cascade has not reached, the closure adds nothing)
+__device__ __forceinline__ float2 add_forcing(float2 fn, const Pointers &p, int kx, int iz, int N)
+{
+    const float g = p.gate ? *p.gate : 1.0f;
+    const float2 f = p.force[(size_t)kx * N + iz];
+    if (p.force_clamp <= 0.0f) return make_float2(fmaf(g, f.x, fn.x), fmaf(g, f.y, fn.y));
+    float fx = g * f.x, fy = g * f.y;
+    const float af = sqrtf(fx * fx + fy * fy), an = p.force_clamp * sqrtf(fn.x * fn.x + fn.y * fn.y);
+    if (af > an) {
+        const float sc = an / af;
+        fx *= sc;
+        fy *= sc;
+    }
+    return make_float2(fn.x + fx, fn.y + fy);
+}
 
 // CFL contribution |u|/DX + |w|/DZ with IEEE division/addition (cuda/dns_cuda.cu:497-502)
 __device__ __forceinline__ float cfl_term(float u, float w, float dx)
@@ -292,12 +312,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
-            if (p.force) {
-                const float g = p.gate ? *p.gate : 1.0f;
-                const float2 f = p.force[(size_t)kx * N + iz];
-                fn.x += g * f.x;
-                fn.y += g * f.y;
-            }
+            if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;
@@ -566,12 +581,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p0, int 
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
-            if (p.force) {
-                const float g = p.gate ? *p.gate : 1.0f;
-                const float2 f = p.force[(size_t)kx * N + iz];
-                fn.x += g * f.x;
-                fn.y += g * f.y;
-            }
+            if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;
@@ -762,12 +772,7 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, 1) k_cols_step4(Pointers p0, 
             const float g2a2 = (float)kz * (float)kz - (float)kx * (float)kx;
             fn.x = (ga * d.x + g2a2 * e.x) * divxz;
             fn.y = (ga * d.y + g2a2 * e.y) * divxz;
-            if (p.force) {
-                const float gt = p.gate ? *p.gate : 1.0f;
-                const float2 f = p.force[(size_t)kx * N + iz];
-                fn.x += gt * f.x;
-                fn.y += gt * f.y;
-            }
+            if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
         const double arg = hvdt * K2;

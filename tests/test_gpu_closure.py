@@ -188,3 +188,31 @@ def test_tensor_core_forcing_matches_fp32_forcing(pkg):
     assert s.closure_stats()[0] == 10
     s.close()
     net.close()
+
+
+def test_forcing_limiter_bounds_each_mode(pkg):
+    """With closure_clamp(alpha), the forcing a closed step adds to FN (closed FNM1 minus the plain
+    step's FNM1 from the same state) is at most alpha |FN| on every mode, and binds on some."""
+    alpha = 0.5
+    s_p = _state(pkg)
+    s_c = _state(pkg)
+    net = pkg.CNN(3, 8, seed=11)
+    s_c.velocity_phys()
+    s_c.om2phys()
+    sc = np.array([s_c.phys(2).std(), s_c.phys(0).std(), s_c.phys(1).std(), 5.0], dtype=np.float32)
+    s_c.attach_closure(net, sc, energy_check=0)
+    F = s_c.closure_forcing().astype(np.complex128)
+    s_c.closure_clamp(alpha)
+    s_p.step(1)
+    s_c.step(1)
+    fn = s_p.fnm1().astype(np.complex128)
+    applied = s_c.fnm1().astype(np.complex128) - fn
+    tol = 1e-6 * (np.abs(fn).max() + np.abs(F).max())
+    assert np.all(np.abs(applied) <= alpha * np.abs(fn) * (1 + 1e-5) + tol)
+    limited = np.abs(F) > alpha * np.abs(fn) * 1.01 + tol
+    assert limited.any()
+    # where it does not bind, the forcing is applied unchanged
+    free = np.abs(F) < alpha * np.abs(fn) * 0.99
+    assert np.abs(applied[free] - F[free]).max() <= tol
+    for x in (s_p, s_c, net):
+        x.close()
