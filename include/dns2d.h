@@ -116,6 +116,17 @@ int dns2d_set_velocity_phys(dns2d_state *s, const float *u, const float *w);
 int dns2d_save_restart(dns2d_state *s, const char *path);
 int dns2d_load_restart(dns2d_state *s, const char *path);
 
+/* ---- movie frames (cuda/color_cuda.cu:491-597, dnsCudaMovieScaleF / dnsCudaSaveFieldInfernoPng
+ * without the PNG file: the CLI writes it) ----
+ * dns2d_movie_scale: the downsampling factor F the reference uses for size N.
+ * dns2d_movie_frame: inferno RGB image (rows of width * 3 bytes) of physical plane comp (0..2; 2 is
+ * the vorticity after dns2d_om2phys), every F-th point of the 3N/2 x 3N/2 grid (F <= 0 means 1).
+ * With rgb NULL only width/height are returned; sigma_out (nullable) receives the plane's pixel
+ * sigma that sets the contrast stretch. */
+int dns2d_movie_scale(int N);
+int dns2d_movie_frame(dns2d_state *s, int comp, int scale_f, unsigned char *rgb, int *width, int *height,
+                      double *sigma_out);
+
 /* ---- time step without device allocation (no counterpart in the reference) ----
  * For callers that cannot allocate device memory: an application that hands out only its own
  * pooled or arena buffers, a process under a fixed device-memory budget, or code where

@@ -43,6 +43,7 @@ SYMBOLS = [
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
+    "dns2d_movie_scale", "dns2d_movie_frame",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -164,6 +165,9 @@ def lib():
         "dns2d_batch_autotune": (C.c_int, [vp]),
         "dns2d_closure_clamp": (C.c_int, [vp, C.c_float]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+        "dns2d_movie_scale": (C.c_int, [C.c_int]),
+        "dns2d_movie_frame": (C.c_int, [vp, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -373,6 +377,18 @@ class Solver:
         out = np.zeros((self.N, self.H), dtype=np.complex64)
         self._chk(self._L.dns2d_closure_forcing(self._s, _fp(out.view(np.float32))))
         return out
+
+    def movie_frame(self, comp: int = 2, scale_f: int = 0):
+        """Inferno RGB frame of physical plane comp (uint8 [h][w][3]) and the plane's pixel sigma;
+        scale_f 0 = the reference's factor for this N."""
+        F = scale_f or self._L.dns2d_movie_scale(self.N)
+        w, h = C.c_int(0), C.c_int(0)
+        self._chk(self._L.dns2d_movie_frame(self._s, comp, F, None, C.byref(w), C.byref(h), None))
+        out = np.zeros((h.value, w.value, 3), dtype=np.uint8)
+        sig = C.c_double(0)
+        self._chk(self._L.dns2d_movie_frame(self._s, comp, F, out.ctypes.data_as(C.c_void_p), C.byref(w),
+                                            C.byref(h), C.byref(sig)))
+        return out, sig.value
 
     def closure_clamp(self, alpha: float):
         """Limit each mode's closure forcing to alpha |FN| (0: off)."""

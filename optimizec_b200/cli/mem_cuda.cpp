@@ -19,6 +19,7 @@
 #include <cmath>
 #include <csignal>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
@@ -26,6 +27,7 @@
 #include <thread>
 #include <vector>
 
+#include <dirent.h>
 #include <sys/stat.h>
 
 namespace {
@@ -109,6 +111,198 @@ bool make_dir(const std::string &path)
 }
 
 std::string join(const std::string &a, const char *b) { return a + "/" + b; }
+
+// ---------------------------------------------------------------------------------------
+// movie frames (cuda/mem_cuda.cu:245-330, :1834-1846, :1899-1910; cuda/color_cuda.cu:269-375)
+// ---------------------------------------------------------------------------------------
+
+// "MOV" among the optional arguments enables frames unless the MOV variable says otherwise;
+// without the argument the MOV variable alone decides (cuda/mem_cuda.cu:245-255)
+bool mov_flag(int argc, char **argv, int first)
+{
+    const char *raw = std::getenv("MOV");
+    for (int i = first; i < argc; ++i)
+        if (iequals(argv[i], "MOV")) raw = (raw && raw[0]) ? raw : "1";
+    return flag_on(raw);
+}
+
+bool make_dirs(const std::string &path)
+{
+    for (size_t p = 1; p <= path.size(); ++p) {
+        if (p < path.size() && path[p] != '/') continue;
+        const std::string part = path.substr(0, p);
+        if (mkdir(part.c_str(), 0775) != 0 && errno != EEXIST) {
+            std::fprintf(stderr, "Failed to create movie folder %s: %s\n", part.c_str(), std::strerror(errno));
+            return false;
+        }
+    }
+    return true;
+}
+
+// <MOV_DIR or ./movies>/cuda_<N>_<K0>_<Re>_<CFL %.3f>_U<UPDATE>
+std::string movie_folder_name(int N, float K0, float Re, float CFL, int update)
+{
+    const char *root = std::getenv("MOV_DIR");
+    char cfl[64];
+    std::snprintf(cfl, sizeof(cfl), "%.3f", (double)CFL);
+    return std::string(root && root[0] ? root : "movies") + "/cuda_" + std::to_string(N) + "_" +
+           std::to_string((int)K0) + "_" + sci_no_plus(Re) + "_" + cfl + "_U" + std::to_string(update);
+}
+
+// highest k among the folder's omega_inferno_<digits>.png files, 0 when there are none: a continued
+// run appends frames after the ones already there
+int last_movie_frame(const std::string &folder)
+{
+    DIR *d = opendir(folder.c_str());
+    if (!d) return 0;
+    static const char pre[] = "omega_inferno_", suf[] = ".png";
+    const size_t lp = sizeof(pre) - 1, ls = sizeof(suf) - 1;
+    int last = 0;
+    while (const dirent *e = readdir(d)) {
+        const std::string n(e->d_name);
+        if (n.size() <= lp + ls || n.compare(0, lp, pre) != 0 || n.compare(n.size() - ls, ls, suf) != 0) continue;
+        const std::string digits = n.substr(lp, n.size() - lp - ls);
+        if (!std::all_of(digits.begin(), digits.end(), [](char c) { return std::isdigit((unsigned char)c) != 0; }))
+            continue;
+        last = std::max(last, std::atoi(digits.c_str()));
+    }
+    closedir(d);
+    return last;
+}
+
+// PNG (ISO/IEC 15948) RGB8 image: filter byte 0 per row, zlib stream (RFC 1950) of stored deflate
+// blocks (RFC 1951 BTYPE 00), one IDAT chunk. CRC-32 is the reflected 0xEDB88320 polynomial,
+// table-driven; Adler-32 defers the modulo over runs of 5552 bytes, the longest run for which
+// the 32-bit sums cannot overflow.
+class PngWriter {
+  public:
+    PngWriter()
+    {
+        for (uint32_t n = 0; n < 256; ++n) {
+            uint32_t c = n;
+            for (int k = 0; k < 8; ++k) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+            crc_table_[n] = c;
+        }
+    }
+
+    bool write(const std::string &path, int w, int h, const unsigned char *rgb) const
+    {
+        const size_t row = (size_t)w * 3 + 1, raw = row * (size_t)h;
+        const size_t nblk = std::max<size_t>(1, (raw + 65534) / 65535);
+        std::vector<unsigned char> z;
+        z.reserve(2 + raw + 5 * nblk + 4);
+        z.push_back(0x78);  // CM 8 (deflate), 32 KB window
+        z.push_back(0x01);  // no preset dictionary, FCHECK so that 0x7801 % 31 == 0
+        uint32_t a = 1, b = 0;
+        size_t done = 0, y = 0, x = 0;  // x: byte within the current row (0 = filter byte)
+        for (size_t k = 0; k < nblk; ++k) {
+            const size_t n = std::min<size_t>(65535, raw - done);
+            z.push_back(k + 1 == nblk ? 1 : 0);
+            z.push_back((unsigned char)(n & 255));
+            z.push_back((unsigned char)(n >> 8));
+            z.push_back((unsigned char)(~n & 255));
+            z.push_back((unsigned char)((~n >> 8) & 255));
+            for (size_t left = n; left > 0;) {
+                if (x == 0) {  // filter type 0 (None) opens each row
+                    z.push_back(0);
+                    b = (b + a) % 65521u;  // adler of a zero byte: a unchanged
+                    --left;
+                    x = 1;
+                    continue;
+                }
+                const size_t take = std::min(left, row - x);
+                const unsigned char *src = rgb + y * (size_t)w * 3 + (x - 1);
+                z.insert(z.end(), src, src + take);
+                adler(src, take, a, b);
+                left -= take;
+                x += take;
+                if (x == row) {
+                    x = 0;
+                    ++y;
+                }
+            }
+            done += n;
+        }
+        put32(z, (b << 16) | a);
+
+        FILE *fp = std::fopen(path.c_str(), "wb");
+        if (!fp) {
+            std::fprintf(stderr, "PNG %s: %s\n", path.c_str(), std::strerror(errno));
+            return false;
+        }
+        static const unsigned char sig[8] = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1A, '\n'};
+        std::vector<unsigned char> ihdr;
+        put32(ihdr, (uint32_t)w);
+        put32(ihdr, (uint32_t)h);
+        ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // depth 8, truecolour, deflate, filter 0, no interlace
+        bool ok = std::fwrite(sig, 1, 8, fp) == 8 && chunk(fp, "IHDR", ihdr) && chunk(fp, "IDAT", z) &&
+                  chunk(fp, "IEND", {});
+        ok = (std::fclose(fp) == 0) && ok;
+        if (!ok) std::fprintf(stderr, "PNG %s: write failed\n", path.c_str());
+        return ok;
+    }
+
+  private:
+    uint32_t crc_table_[256];
+
+    static void put32(std::vector<unsigned char> &v, uint32_t x)
+    {
+        for (int s = 24; s >= 0; s -= 8) v.push_back((unsigned char)(x >> s));
+    }
+
+    // a and b enter and leave reduced mod 65521
+    static void adler(const unsigned char *p, size_t n, uint32_t &a, uint32_t &b)
+    {
+        while (n > 0) {
+            const size_t run = std::min<size_t>(n, 5552);
+            for (size_t i = 0; i < run; ++i) {
+                a += p[i];
+                b += a;
+            }
+            a %= 65521u;
+            b %= 65521u;
+            p += run;
+            n -= run;
+        }
+    }
+
+    uint32_t crc(uint32_t c, const unsigned char *p, size_t n) const
+    {
+        for (size_t i = 0; i < n; ++i) c = crc_table_[(c ^ p[i]) & 255u] ^ (c >> 8);
+        return c;
+    }
+
+    bool chunk(FILE *fp, const char type[5], const std::vector<unsigned char> &data) const
+    {
+        std::vector<unsigned char> head;
+        put32(head, (uint32_t)data.size());
+        head.insert(head.end(), type, type + 4);
+        uint32_t c = crc(0xFFFFFFFFu, head.data() + 4, 4);
+        c = crc(c, data.data(), data.size()) ^ 0xFFFFFFFFu;
+        std::vector<unsigned char> tail;
+        put32(tail, c);
+        return std::fwrite(head.data(), 1, 8, fp) == 8 &&
+               (data.empty() || std::fwrite(data.data(), 1, data.size(), fp) == data.size()) &&
+               std::fwrite(tail.data(), 1, 4, fp) == 4;
+    }
+};
+
+// one frame of the vorticity plane (comp 2 of the physical planes, filled by dns2d_om2phys)
+bool save_movie_frame(dns2d_state *s, const PngWriter &png, const std::string &path, int F)
+{
+    int w = 0, h = 0;
+    double sigma = 0.0;
+    dns2d_movie_frame(s, 2, F, nullptr, &w, &h, nullptr);
+    std::vector<unsigned char> rgb((size_t)w * h * 3);
+    const int rc = dns2d_movie_frame(s, 2, F, rgb.data(), &w, &h, &sigma);
+    if (rc) {
+        std::fprintf(stderr, "dns2d_movie_frame failed: %s (%s)\n", dns2d_strerror(rc), dns2d_last_error(s));
+        return false;
+    }
+    if (!png.write(path, w, h, rgb.data())) return false;
+    std::printf("[MOV] Wrote %s (Inferno PNG, %dx%d, F=%d, comp=%d, sigma=%d)\n", path.c_str(), w, h, F, 2, (int)sigma);
+    return true;
+}
 
 void die(dns2d_state *s, int rc, const char *what)
 {
@@ -489,9 +683,7 @@ int main(int argc, char **argv)
         const char *e = std::getenv("RESTART_STEPS");
         if (e && e[0]) STEPS = std::atoi(e);
         RESTART_PATH = restart_storage.c_str();
-        MOV = flag_on(std::getenv("MOV"));
-        for (int i = 3; i < argc; ++i)
-            if (iequals(argv[i], "MOV")) MOV = true;
+        MOV = mov_flag(argc, argv, 3);
     } else {
         if (argc > 1) N = std::atoi(argv[1]);
         if (argc > 2) Re = (float)std::atof(argv[2]);
@@ -505,9 +697,7 @@ int main(int argc, char **argv)
             RESTART_PATH = argv[8];
             mov_begin = 9;
         }
-        MOV = flag_on(std::getenv("MOV"));
-        for (int i = mov_begin; i < argc; ++i)
-            if (iequals(argv[i], "MOV")) MOV = true;
+        MOV = mov_flag(argc, argv, mov_begin);
     }
     if (UPDATE <= 0) UPDATE = 100;
     if (STEPS <= 0) STEPS = 1000000;
@@ -518,7 +708,6 @@ int main(int argc, char **argv)
                 (double)CFL, UPDATE, ADAPT ? 1 : 0, MOV ? 1 : 0);
     if (phase_timing) std::printf("[PHASE] PHASE_TIMING enabled; profiling will synchronize measured phases.\n");
     if (RESTART_PATH) std::printf(" restart=%s\n", RESTART_PATH);
-    if (MOV) std::printf("[MOV] movie frames are not produced by this build; continuing without them.\n");
     gpu_snapshot("start");
 
     dns2d_state *s = nullptr;
@@ -607,6 +796,20 @@ int main(int argc, char **argv)
         std::printf("[BENCH] Steady FPS timer starts immediately (BENCH_WARMUP_STEPS=0).\n");
     }
     auto elapsed_active = [&]() { return std::chrono::duration<double>(clk::now() - tbegin).count() - paused; };
+    const int movie_F = dns2d_movie_scale(N);
+    std::string movie_folder;
+    int movie_frame = 0;
+    const PngWriter png;
+    if (MOV) {
+        movie_folder = movie_folder_name(N, K0, Re, CFL, UPDATE);
+        if (!make_dirs(movie_folder)) {
+            dns2d_destroy(s);
+            return 1;
+        }
+        movie_frame = last_movie_frame(movie_folder);
+        std::printf("[MOV] Saving omega_inferno_%%05d.png every %d steps to %s (F=%d, next=%05d)\n", UPDATE,
+                    movie_folder.c_str(), movie_F, movie_frame + 1);
+    }
     auto is_diag = [&](int it) { return it == 1 || it % UPDATE == 0 || it == STEPS; };
 
     int it = sc.it;
@@ -643,6 +846,15 @@ int main(int argc, char **argv)
                         "FPS=%.3f\n",
                         it, (double)sc.t, (double)sc.dt, (double)sc.cn, (double)sc.cflm, (double)sc.Re, (double)sc.visc,
                         rows.back().PALIN, rows.back().SIG, rows.back().FPS);
+            if (MOV && it > 0 && it % UPDATE == 0) {
+                char name[64];
+                std::snprintf(name, sizeof(name), "omega_inferno_%05d.png", movie_frame + 1);
+                if (!save_movie_frame(s, png, join(movie_folder, name), movie_F)) {
+                    dns2d_destroy(s);
+                    return 1;
+                }
+                ++movie_frame;
+            }
             if (!steady_started && it >= warm) {
                 dns2d_sync(s, 0);
                 steady_begin = clk::now();

@@ -1177,6 +1177,186 @@ extern "C" int dns2d_next_dt(dns2d_state *s, float *cflm_out)
 }
 
 // ============================================================================================
+// movie frames: inferno colour map of a physical plane (cuda/color_cuda.cu:37-232, :491-597)
+// ============================================================================================
+namespace {
+
+__constant__ unsigned char c_inferno[256 * 3];
+
+// five colour stops, linear in between, truncated to bytes (cuda/color_cuda.cu:37-70)
+void inferno_lut(unsigned char lut[768])
+{
+    const float pos[5] = {0.00f, 0.25f, 0.50f, 0.75f, 1.00f};
+    const unsigned char col[5][3] = {{0, 0, 4}, {87, 15, 109}, {187, 55, 84}, {249, 142, 8}, {252, 255, 164}};
+    for (int i = 0; i < 256; ++i) {
+        const float x = (float)i / 255.0f;
+        int k = 0;
+        while (k + 1 < 5 && x > pos[k + 1]) ++k;
+        const int k1 = std::min(k + 1, 4);
+        const float span = std::max(1.0e-12f, pos[k1] - pos[k]);
+        const float t = std::max(0.0f, std::min(1.0f, (x - pos[k]) / span));
+        for (int c = 0; c < 3; ++c) lut[3 * i + c] = (unsigned char)((1.0f - t) * col[k][c] + t * col[k1][c]);
+    }
+}
+
+constexpr int kFrameBlocks = 1024;
+
+// per-block min/max over the finite values
+__global__ void k_frame_minmax(const float *f, size_t n, float2 *out)
+{
+    __shared__ float smn[256], smx[256];
+    float mn = 3.402823466e38f, mx = -3.402823466e38f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = f[i];
+        if (isfinite(v)) {
+            mn = fminf(mn, v);
+            mx = fmaxf(mx, v);
+        }
+    }
+    smn[threadIdx.x] = mn;
+    smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            smn[threadIdx.x] = fminf(smn[threadIdx.x], smn[threadIdx.x + o]);
+            smx[threadIdx.x] = fmaxf(smx[threadIdx.x], smx[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = make_float2(smn[0], smx[0]);
+}
+
+// pixel value 1..255 of v (cuda/color_cuda.cu:150-160); 1 + 254 norm is one fused multiply-add, as the
+// reference's nvcc build contracts it
+__device__ __forceinline__ int frame_pixel(float v, float minv, float inv_range, int is_constant)
+{
+    if (is_constant || !isfinite(v)) return 128;
+    const float norm = (v - minv) * inv_range;
+    float pf = fmaf(norm, 254.0f, 1.0f);
+    if (pf < 1.0f) pf = 1.0f;
+    if (pf > 255.0f) pf = 255.0f;
+    return (int)pf;
+}
+
+// per-block sums of pix and pix^2 (integers: exact in FP64, independent of the order)
+__global__ void k_frame_stats(const float *f, size_t n, float minv, float inv_range, int is_constant, double2 *out)
+{
+    __shared__ double s1[256], s2[256];
+    double a = 0.0, b = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double p = (double)frame_pixel(f[i], minv, inv_range, is_constant);
+        a += p;
+        b += p * p;
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = make_double2(s1[0], s2[0]);
+}
+
+// one output pixel per thread, sampling every F-th point; the colour index stretches
+// [mean - 2.5 sigma, mean + 2.5 sigma] of the pixel values over the table when sigma >= 1
+// rows [oy0, oy1) of the frame, written from rgb[0]
+__global__ void k_frame_render(const float *f, unsigned char *rgb, int nx, int nz, int out_w, int oy0, int oy1, int F,
+                               float minv, float inv_range, int is_constant, double mean, double sigma)
+{
+    const int ox = blockIdx.x * blockDim.x + threadIdx.x, oy = oy0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= out_w || oy >= oy1) return;
+    const int x = min(ox * F, nx - 1), y = min(oy * F, nz - 1);
+    const int pix = frame_pixel(f[(size_t)y * nx + x], minv, inv_range, is_constant);
+    int ci = pix;
+    const double lo = mean - 2.5 * sigma, hi = mean + 2.5 * sigma;
+    if (sigma >= 1.0 && hi > lo) {
+        ci = (int)floor(((double)pix - lo) * 255.0 / (hi - lo) + 0.5);
+        ci = ci < 0 ? 0 : (ci > 255 ? 255 : ci);
+    }
+    const size_t d = 3 * ((size_t)(oy - oy0) * out_w + ox);
+    rgb[d] = c_inferno[3 * ci];
+    rgb[d + 1] = c_inferno[3 * ci + 1];
+    rgb[d + 2] = c_inferno[3 * ci + 2];
+}
+
+}  // namespace
+
+// frame downsampling factor for size N (cuda/color_cuda.cu:491-498)
+extern "C" int dns2d_movie_scale(int N)
+{
+    if (N == 9216) return 8;
+    if (N == 16384) return 12;
+    if (N == 29400) return 14;
+    return std::max(1, (3 * N / 2 + 3839) / 3840);
+}
+
+extern "C" int dns2d_movie_frame(dns2d_state *s, int comp, int scale_f, unsigned char *rgb, int *width, int *height,
+                                 double *sigma_out)
+{
+    if (!s || comp < 0 || comp > 2) return DNS2D_ERR_ARG;
+    const int F = scale_f > 0 ? scale_f : 1;
+    const int L = s->L;
+    const int out_w = (L + F - 1) / F, out_h = (L + F - 1) / F;
+    if (width) *width = out_w;
+    if (height) *height = out_h;
+    if (!rgb) return DNS2D_OK;
+    const size_t plane = (size_t)L * L;
+    const float *f = s->phys + (size_t)comp * plane;
+    const int nb = (int)std::min<size_t>(kFrameBlocks, std::max<size_t>(1, (plane + 255) / 256));
+    static_assert(kFrameBlocks <= kSigmaBlocks, "frame partials share the sigma buffers");
+    k_frame_minmax<<<nb, 256, 0, s->stream>>>(f, plane, s->minmax);
+    DNS2D_LAUNCHED("frame minmax");
+    std::vector<float2> mm((size_t)nb);
+    DNS2D_CUDA(cudaMemcpyAsync(mm.data(), s->minmax, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->stream), "minmax copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "minmax sync");
+    float minv = mm[0].x, maxv = mm[0].y;
+    for (int i = 1; i < nb; ++i) {
+        minv = std::min(minv, mm[(size_t)i].x);
+        maxv = std::max(maxv, mm[(size_t)i].y);
+    }
+    const float range = maxv - minv;
+    const int is_constant = !(range > 1.0e-12f);
+    const float inv_range = is_constant ? 1.0f : 1.0f / range;
+    double2 *sums = reinterpret_cast<double2 *>(s->sums);
+    k_frame_stats<<<nb, 256, 0, s->stream>>>(f, plane, minv, inv_range, is_constant, sums);
+    DNS2D_LAUNCHED("frame stats");
+    std::vector<double2> st((size_t)nb);
+    DNS2D_CUDA(cudaMemcpyAsync(st.data(), sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, s->stream), "stats copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "stats sync");
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < nb; ++i) {
+        a += st[(size_t)i].x;
+        b += st[(size_t)i].y;
+    }
+    const double mean = a / (double)plane;
+    const double sigma = std::sqrt(std::max(0.0, b / (double)plane - mean * mean));
+    if (sigma_out) *sigma_out = sigma;
+    unsigned char lut[768];
+    inferno_lut(lut);
+    DNS2D_CUDA(cudaMemcpyToSymbolAsync(c_inferno, lut, sizeof(lut), 0, cudaMemcpyHostToDevice, s->stream), "lut copy");
+    // the frame goes through the scratch buffer (8 L H bytes) in bands of rows: at F = 1 the whole
+    // frame (3 L^2 bytes) is larger than the buffer
+    unsigned char *d_rgb = reinterpret_cast<unsigned char *>(s->scratch);
+    const int band = (int)std::min<size_t>(out_h, (size_t)8 * L * s->H / ((size_t)3 * out_w));
+    for (int oy0 = 0; oy0 < out_h; oy0 += band) {
+        const int oy1 = std::min(out_h, oy0 + band);
+        const dim3 blk(16, 16), grd((out_w + 15) / 16, (oy1 - oy0 + 15) / 16);
+        k_frame_render<<<grd, blk, 0, s->stream>>>(f, d_rgb, L, L, out_w, oy0, oy1, F, minv, inv_range, is_constant,
+                                                   mean, sigma);
+        DNS2D_LAUNCHED("movie frame");
+        DNS2D_CUDA(cudaMemcpyAsync(rgb + (size_t)3 * out_w * oy0, d_rgb, (size_t)3 * out_w * (oy1 - oy0),
+                                   cudaMemcpyDeviceToHost, s->stream),
+                   "rgb copy");
+    }
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "rgb sync");
+    return DNS2D_OK;
+}
+
+// ============================================================================================
 // diagnostics
 // ============================================================================================
 extern "C" int dns2d_om2phys(dns2d_state *s)

@@ -127,6 +127,72 @@ def display_sigma(field: np.ndarray) -> float:
     return lib().orc_display_sigma(_dp(f), f.size)
 
 
+def movie_scale(N: int) -> int:
+    """Frame downsampling factor for size N (cuda/color_cuda.cu:491-498)."""
+    return {9216: 8, 16384: 12, 29400: 14}.get(N, max(1, (3 * N // 2 + 3839) // 3840))
+
+
+def inferno_lut() -> np.ndarray:
+    """256x3 colour table: five stops, linear in between, float32 arithmetic truncated to bytes
+    (cuda/color_cuda.cu:37-70)."""
+    pos = np.array([0.0, 0.25, 0.5, 0.75, 1.0], dtype=np.float32)
+    col = np.array([[0, 0, 4], [87, 15, 109], [187, 55, 84], [249, 142, 8], [252, 255, 164]], dtype=np.float32)
+    lut = np.zeros((256, 3), dtype=np.uint8)
+    for i in range(256):
+        x = np.float32(i) / np.float32(255)
+        k = 0
+        while k + 1 < 5 and x > pos[k + 1]:
+            k += 1
+        k1 = min(k + 1, 4)
+        span = max(np.float32(1e-12), pos[k1] - pos[k])
+        t = np.float32(min(np.float32(1), max(np.float32(0), (x - pos[k]) / span)))
+        for c in range(3):
+            v = (np.float32(1) - t) * col[k, c] + t * col[k1, c]
+            lut[i, c] = int(np.float32(v))
+    return lut
+
+
+def frame_pixels(field: np.ndarray) -> np.ndarray:
+    """Pixel values 1..255 of a float32 plane (cuda/color_cuda.cu:95-185, :518-540): min/max over
+    the finite values, pix = trunc(clamp(1 + 254 norm)) with 1 + 254 norm one fused multiply-add as
+    the device computes it, 128 for non-finite values and for a constant plane."""
+    f = np.ascontiguousarray(field, dtype=np.float32)
+    fin = np.isfinite(f)
+    if not fin.any():
+        return np.full(f.shape, 128, dtype=np.int64)
+    minv, maxv = np.float32(f[fin].min()), np.float32(f[fin].max())
+    rng = np.float32(maxv - minv)
+    if not rng > np.float32(1e-12):
+        return np.full(f.shape, 128, dtype=np.int64)
+    inv = np.float32(np.float32(1) / rng)
+    with np.errstate(invalid="ignore", over="ignore"):
+        norm = (f - minv).astype(np.float32) * inv                      # two float32 roundings
+        pf = (norm.astype(np.float64) * 254.0 + 1.0).astype(np.float32)  # one rounding: fma(norm, 254, 1)
+        pf = np.clip(pf, np.float32(1), np.float32(255))
+        return np.where(fin, np.trunc(np.nan_to_num(pf)), 128).astype(np.int64)
+
+
+def render_frame(field: np.ndarray, F: int):
+    """Inferno RGB frame (uint8 [h][w][3]) of a float32 plane sampled every F points, and the
+    plane's pixel sigma (cuda/color_cuda.cu:186-232, :500-597): colour index = pix, or
+    round((pix - lo) * 255 / (hi - lo)) clamped to [0, 255] with lo/hi = mean -/+ 2.5 sigma of all
+    pixels when sigma >= 1."""
+    pix = frame_pixels(field)
+    n = pix.size
+    mean = float(pix.sum()) / n
+    sigma = float(np.sqrt(max(0.0, float((pix * pix).sum()) / n - mean * mean)))
+    nz, nx = pix.shape
+    oh, ow = (nz + F - 1) // F, (nx + F - 1) // F
+    ys = np.minimum(np.arange(oh) * F, nz - 1)
+    xs = np.minimum(np.arange(ow) * F, nx - 1)
+    p = pix[np.ix_(ys, xs)]
+    ci = p.copy()
+    lo, hi = mean - 2.5 * sigma, mean + 2.5 * sigma
+    if sigma >= 1.0 and hi > lo:
+        ci = np.clip(np.floor((p.astype(np.float64) - lo) * 255.0 / (hi - lo) + 0.5), 0, 255).astype(np.int64)
+    return inferno_lut()[ci], sigma
+
+
 def threads() -> int:
     return lib().orc_threads()
 

@@ -112,3 +112,12 @@ def test_oracle_energy_history_is_monotone_decay():
     E, Z, _ = o.run(20, 100, 20)
     assert np.all(np.diff(E) < 0)  # 2D decaying turbulence: energy decays monotonically
     assert np.all(Z > 0)
+
+
+def test_movie_restatement_rules():
+    """Colour table stops, the reference's per-size downsampling factors, constant planes."""
+    lut = O.inferno_lut()
+    assert lut[0].tolist() == [0, 0, 4] and lut[255].tolist() == [252, 255, 164]
+    assert [O.movie_scale(n) for n in (256, 2560, 4096, 9216, 16384, 29400)] == [1, 1, 2, 8, 12, 14]
+    rgb, sigma = O.render_frame(np.full((12, 12), 3.0, np.float32), 5)
+    assert rgb.shape == (3, 3, 3) and sigma == 0.0 and np.all(rgb == lut[128])
