@@ -14,6 +14,7 @@
 #include "../../include/dns2d.h"
 
 #include <algorithm>
+#include <cerrno>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -21,11 +22,16 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 using namespace dns2d;
 
@@ -451,6 +457,9 @@ struct dns2d_state {
     int hist_cap = 0;
     // pinned host
     double2 *hist_host = nullptr;
+    unsigned char *stage = nullptr;  // restart file staging: kStageBufs buffers of stage_chunk bytes
+    size_t stage_chunk = 0;
+    cudaEvent_t stage_ev[3] = {nullptr, nullptr, nullptr};
     // graphs keyed by (first, K)
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     // phase timing
@@ -699,6 +708,9 @@ extern "C" void dns2d_destroy(dns2d_state *s)
     cudaFree(s->bk_work);
     cudaFree(s->closure_in);
     if (s->hist_host) cudaFreeHost(s->hist_host);
+    if (s->stage) cudaFreeHost(s->stage);
+    for (cudaEvent_t e : s->stage_ev)
+        if (e) cudaEventDestroy(e);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1609,6 +1621,94 @@ static_assert(sizeof(RestartV2) == 144, "restart v2 header size");
 
 }  // namespace
 
+namespace {
+
+// Restart files move through pinned staging buffers: file chunk k (stage_chunk bytes from the
+// start of the payload range) lives in buffer k % kStageBufs. Saving keeps kStageBufs
+// device->host copies in flight while the host writes the oldest finished chunk; loading reads
+// chunk k from the file (kReadThreads preads in parallel) while the host->device copies of the
+// chunks before it run. Each region of the file is one contiguous device range, so a chunk is at
+// most a few cudaMemcpyAsync calls; the file's [iz][ix] OM2/FNM1 and the state's [ix][iz] are
+// transposed on the device, one array at a time through the scratch buffer.
+constexpr int kStageBufs = 3;
+constexpr size_t kStageChunkMax = 64ull << 20;
+constexpr int kReadThreads = 4;
+
+// file bytes [off, off + len) are dev[0, len) (or host[0, len) for the header); `before` (save)
+// is enqueued ahead of the region's first copy, `after` (load) behind its last
+struct FileRegion {
+    uint64_t off, len;
+    unsigned char *dev;
+    const unsigned char *host;
+    std::function<void()> before, after;
+};
+
+int stage_reserve(dns2d_state *s, uint64_t bytes)
+{
+    const size_t want = std::min<size_t>(
+        kStageChunkMax, std::max<size_t>(4096, ((bytes + kStageBufs - 1) / kStageBufs + 4095) / 4096 * 4096));
+    if (s->stage && s->stage_chunk >= want) return DNS2D_OK;
+    if (s->stage) cudaFreeHost(s->stage);
+    s->stage = nullptr;
+    s->stage_chunk = 0;
+    DNS2D_CUDA(cudaHostAlloc((void **)&s->stage, want * kStageBufs, cudaHostAllocDefault), "staging buffers");
+    s->stage_chunk = want;
+    for (cudaEvent_t &e : s->stage_ev)
+        if (!e) DNS2D_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "staging events");
+    return DNS2D_OK;
+}
+
+bool write_all(int fd, const unsigned char *p, size_t n)
+{
+    while (n > 0) {
+        const ssize_t w = ::write(fd, p, std::min<size_t>(n, 1ull << 30));
+        if (w < 0 && errno == EINTR) continue;
+        if (w <= 0) return false;
+        p += w;
+        n -= (size_t)w;
+    }
+    return true;
+}
+
+bool pread_all(int fd, unsigned char *p, size_t n, uint64_t off)
+{
+    while (n > 0) {
+        const ssize_t r = ::pread(fd, p, std::min<size_t>(n, 1ull << 30), (off_t)off);
+        if (r < 0 && errno == EINTR) continue;
+        if (r <= 0) return false;
+        p += r;
+        n -= (size_t)r;
+        off += (uint64_t)r;
+    }
+    return true;
+}
+
+// file bytes [lo, hi) into buf, by up to kReadThreads threads reading contiguous slices
+bool pread_parallel(int fd, unsigned char *buf, uint64_t lo, uint64_t hi)
+{
+    const uint64_t n = hi - lo;
+    const int t = n >= (8ull << 20) ? kReadThreads : 1;
+    if (t == 1) return pread_all(fd, buf, n, lo);
+    const uint64_t part = (n + t - 1) / t;
+    bool ok[kReadThreads];
+    std::vector<std::thread> th;
+    for (int i = 0; i < t; ++i) {
+        const uint64_t a = std::min<uint64_t>(n, i * part), b = std::min<uint64_t>(n, a + part);
+        ok[i] = true;
+        th.emplace_back([&ok, fd, buf, lo, i, a, b] { ok[i] = pread_all(fd, buf + a, b - a, lo + a); });
+    }
+    for (auto &x : th) x.join();
+    return std::all_of(ok, ok + t, [](bool v) { return v; });
+}
+
+void transpose_c64(dns2d_state *s, const float2 *in, float2 *out, int rows, int cols)
+{
+    dim3 b(32, 8), g((cols + 31) / 32, (rows + 31) / 32);
+    k_transpose_c64<<<g, b, 0, s->stream>>>(in, out, rows, cols);
+}
+
+}  // namespace
+
 extern "C" int dns2d_save_restart(dns2d_state *s, const char *path)
 {
     if (!s || !path) return DNS2D_ERR_ARG;
@@ -1639,55 +1739,73 @@ extern "C" int dns2d_save_restart(dns2d_state *s, const char *path)
     h.ur_full_count = 3 * n;
     int rc = dns2d_velocity_phys(s);
     if (rc) return rc;
-    std::vector<float> buf(n);
-    FILE *fp = std::fopen(path, "wb");
-    if (!fp) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
-    bool ok = std::fwrite(&h, 1, sizeof(h), fp) == sizeof(h);
-    for (int c = 0; ok && c < 3; ++c) {
-        rc = dns2d_get_phys(s, c, buf.data());
-        if (rc) {
-            std::fclose(fp);
-            return rc;
+    const uint64_t hb = sizeof(h), ur = 3 * n * 4, om = nom * 8, total = hb + ur + 2 * om;
+    unsigned char *scr = reinterpret_cast<unsigned char *>(s->scratch);
+    // file order: header, UR_full (three planes), OM2, FNM1 in [iz][ix]; the scratch buffer holds
+    // OM2 then FNM1 (stream order keeps FNM1's transpose behind OM2's last copy out of it)
+    const FileRegion reg[4] = {
+        {0, hb, nullptr, reinterpret_cast<const unsigned char *>(&h), nullptr, nullptr},
+        {hb, ur, reinterpret_cast<unsigned char *>(s->phys), nullptr, nullptr, nullptr},
+        {hb + ur, om, scr, nullptr, [&] { transpose_c64(s, s->om2, s->scratch, s->H, s->N); }, nullptr},
+        {hb + ur + om, om, scr, nullptr, [&] { transpose_c64(s, s->fnm1, s->scratch, s->H, s->N); }, nullptr},
+    };
+    rc = stage_reserve(s, total);
+    if (rc) return rc;
+    const uint64_t C = s->stage_chunk, nch = (total + C - 1) / C;
+    const int fd = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) return fail(s, DNS2D_ERR_IO, "cannot open %s: %s", path, std::strerror(errno));
+    cudaError_t ce = cudaSuccess;
+    auto enqueue = [&](uint64_t k) {
+        unsigned char *buf = s->stage + (k % kStageBufs) * C;
+        const uint64_t lo = k * C, hi = std::min(total, lo + C);
+        for (const FileRegion &r : reg) {
+            const uint64_t a = std::max(lo, r.off), b = std::min(hi, r.off + r.len);
+            if (a >= b) continue;
+            if (a == r.off && r.before) r.before();
+            if (r.host)
+                std::memcpy(buf + (a - lo), r.host + (a - r.off), b - a);
+            else if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(buf + (a - lo), r.dev + (a - r.off), b - a, cudaMemcpyDeviceToHost, s->stream);
         }
-        ok = std::fwrite(buf.data(), 4, n, fp) == n;
+        if (ce == cudaSuccess) ce = cudaEventRecord(s->stage_ev[k % kStageBufs], s->stream);
+    };
+    bool ok = true;
+    for (uint64_t k = 0; k < std::min<uint64_t>(nch, kStageBufs); ++k) enqueue(k);
+    for (uint64_t k = 0; k < nch && ok && ce == cudaSuccess; ++k) {
+        ce = cudaEventSynchronize(s->stage_ev[k % kStageBufs]);
+        if (ce != cudaSuccess) break;
+        const uint64_t lo = k * C, hi = std::min(total, lo + C);
+        ok = write_all(fd, s->stage + (k % kStageBufs) * C, hi - lo);
+        if (ok && k + kStageBufs < nch) enqueue(k + kStageBufs);  // into the buffer just written
     }
-    std::vector<float> sp(nom * 2);
-    if (ok) {
-        rc = dns2d_get_om2(s, sp.data());
-        if (rc) {
-            std::fclose(fp);
-            return rc;
-        }
-        ok = std::fwrite(sp.data(), 8, nom, fp) == nom;
-    }
-    if (ok) {
-        rc = dns2d_get_fnm1(s, sp.data());
-        if (rc) {
-            std::fclose(fp);
-            return rc;
-        }
-        ok = std::fwrite(sp.data(), 8, nom, fp) == nom;
-    }
-    if (std::fclose(fp) != 0) ok = false;
+    if (ce == cudaSuccess) ce = cudaGetLastError();  // the transposes
+    const cudaError_t se = cudaStreamSynchronize(s->stream);
+    if (::close(fd) != 0) ok = false;
+    if (ce == cudaSuccess) ce = se;
+    if (ce != cudaSuccess) return cuda_check(s, ce, "restart staging");
     return ok ? DNS2D_OK : fail(s, DNS2D_ERR_IO, "write failed: %s", path);
 }
 
 extern "C" int dns2d_load_restart(dns2d_state *s, const char *path)
 {
     if (!s || !path) return DNS2D_ERR_ARG;
-    FILE *fp = std::fopen(path, "rb");
-    if (!fp) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
     RestartV2 h;
     std::memset(&h, 0, sizeof(h));
     auto bad = [&](int code, const char *msg) {
-        std::fclose(fp);
+        ::close(fd);
         return fail(s, code, "%s: %s", path, msg);
     };
-    if (std::fread(&h.v1, 1, sizeof(h.v1), fp) != sizeof(h.v1)) return bad(DNS2D_ERR_IO, "short header");
+    struct stat st;
+    if (fstat(fd, &st) != 0) return bad(DNS2D_ERR_IO, "stat");
+    if (!pread_all(fd, reinterpret_cast<unsigned char *>(&h.v1), sizeof(h.v1), 0))
+        return bad(DNS2D_ERR_IO, "short header");
     if (std::strncmp(h.v1.magic, "CTRB_RESTART", 12) != 0) return bad(DNS2D_ERR_FORMAT, "bad magic");
     if (h.v1.version == 2) {
         if (h.v1.header_bytes != sizeof(RestartV2)) return bad(DNS2D_ERR_FORMAT, "header size");
-        if (std::fread(&h.ur_full_count, 1, 8, fp) != 8) return bad(DNS2D_ERR_IO, "short header");
+        if (!pread_all(fd, reinterpret_cast<unsigned char *>(&h.ur_full_count), 8, sizeof(h.v1)))
+            return bad(DNS2D_ERR_IO, "short header");
     }
     if (h.v1.version < 1 || h.v1.version > 2 || (h.v1.version == 1 && h.v1.header_bytes != sizeof(RestartV1)) ||
         h.v1.real_bytes != 4 || h.v1.cplx_bytes != 8)
@@ -1700,34 +1818,55 @@ extern "C" int dns2d_load_restart(dns2d_state *s, const char *path)
     if ((h.v1.version == 1 && h.v1.uc_full_count != ucn) || (h.v1.version >= 2 && has_uc && h.v1.uc_full_count != ucn) ||
         (h.v1.version >= 2 && h.ur_full_count != urn) || h.v1.om2_count != omn || h.v1.fnm1_count != omn)
         return bad(DNS2D_ERR_FORMAT, "array sizes do not match this run");
-    // UC_full payload (v1, or v2 with one) is skipped: the velocity is rebuilt from UR or OM2
-    if (h.v1.version == 1 || has_uc) {
-        if (std::fseek(fp, (long)(h.v1.uc_full_count * 8), SEEK_CUR) != 0) return bad(DNS2D_ERR_IO, "seek");
+    // the UC_full payload (v1, or v2 with one) is not read: the velocity is rebuilt from UR or OM2
+    const uint64_t hb = h.v1.header_bytes, uc = (h.v1.version == 1 || has_uc) ? h.v1.uc_full_count * 8 : 0;
+    const uint64_t ur = h.v1.version >= 2 ? urn * 4 : 0, om = omn * 8;
+    const uint64_t first = hb + uc, end = first + ur + 2 * om;
+    if ((uint64_t)st.st_size < end) return bad(DNS2D_ERR_IO, "short payload");
+    int rc = stage_reserve(s, end - first);
+    if (rc) {
+        ::close(fd);
+        return rc;
     }
-    const size_t n = (size_t)s->L * s->L;
-    std::vector<float> u, w;
-    if (h.v1.version >= 2) {
-        u.resize(n);
-        w.resize(n);
-        if (std::fread(u.data(), 4, n, fp) != n || std::fread(w.data(), 4, n, fp) != n ||
-            std::fseek(fp, (long)(n * 4), SEEK_CUR) != 0)
-            return bad(DNS2D_ERR_IO, "short UR payload");
+    unsigned char *scr = reinterpret_cast<unsigned char *>(s->scratch);
+    const FileRegion reg[3] = {
+        {first, ur, reinterpret_cast<unsigned char *>(s->phys), nullptr, nullptr, nullptr},
+        {first + ur, om, scr, nullptr, nullptr, [&] { transpose_c64(s, s->scratch, s->om2, s->N, s->H); }},
+        {first + ur + om, om, scr, nullptr, nullptr, [&] { transpose_c64(s, s->scratch, s->fnm1, s->N, s->H); }},
+    };
+    // from here on the device state is overwritten: a failure leaves it without an initial condition
+    s->initialised = false;
+    const uint64_t C = s->stage_chunk, nch = (end - first + C - 1) / C;
+    cudaError_t ce = cudaSuccess;
+    bool ok = true;
+    for (uint64_t k = 0; k < nch && ok && ce == cudaSuccess; ++k) {
+        unsigned char *buf = s->stage + (k % kStageBufs) * C;
+        if (k >= kStageBufs) ce = cudaEventSynchronize(s->stage_ev[k % kStageBufs]);  // its last copies done
+        if (ce != cudaSuccess) break;
+        const uint64_t lo = first + k * C, hi = std::min(end, lo + C);
+        ok = pread_parallel(fd, buf, lo, hi);
+        if (!ok) break;
+        for (const FileRegion &r : reg) {
+            const uint64_t a = std::max(lo, r.off), b = std::min(hi, r.off + r.len);
+            if (a >= b) continue;
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(r.dev + (a - r.off), buf + (a - lo), b - a, cudaMemcpyHostToDevice, s->stream);
+            if (b == r.off + r.len && r.after) r.after();
+        }
+        if (ce == cudaSuccess) ce = cudaEventRecord(s->stage_ev[k % kStageBufs], s->stream);
     }
-    std::vector<float> om(omn * 2), fn(omn * 2);
-    if (std::fread(om.data(), 8, omn, fp) != omn || std::fread(fn.data(), 8, omn, fp) != omn)
-        return bad(DNS2D_ERR_IO, "short OM2/FNM1 payload");
-    std::fclose(fp);
-    int rc = upload_compact(s, om.data(), s->om2);
-    if (rc) return rc;
-    rc = upload_compact(s, fn.data(), s->fnm1);
-    if (rc) return rc;
-    if (h.v1.version >= 2) {
-        rc = dns2d_set_velocity_phys(s, u.data(), w.data());
-    } else {
-        s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream, 1);  // velocity from OM2 (v1)
-        rc = cuda_check(s, cudaStreamSynchronize(s->stream), "v1 velocity");
+    ::close(fd);
+    if (ok && ce == cudaSuccess) {
+        if (h.v1.version >= 2)
+            s->ks->rows_from_phys(s->ptrs(), s->phys, s->stream);
+        else
+            s->ks->cols_init(s->ptrs(), nullptr, 1, s->stream, 1);  // velocity from OM2 (v1)
+        ce = cudaGetLastError();
     }
-    if (rc) return rc;
+    const cudaError_t se = cudaStreamSynchronize(s->stream);
+    if (ce == cudaSuccess) ce = se;
+    if (ce != cudaSuccess) return cuda_check(s, ce, "restart staging");
+    if (!ok) return fail(s, DNS2D_ERR_IO, "%s: read failed", path);
     s->Re = h.v1.Re;
     s->K0 = h.v1.K0;
     s->visc = h.v1.visc;
