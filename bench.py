@@ -31,8 +31,10 @@ sys.path.insert(0, REPO)
 
 # dns4096: the headline configuration.  dns29400: the large run of the reference's README
 # (mem_cuda 29400 1E7 4 41 0.1 20 0: 41 steps, its Steady FPS after 20 warm-up steps).
+# dns16384: the reference's recorded N=16384 run (mem_cuda 16384 1E6 5 21 0.2 10 0), with 41 steps.
 WORKLOADS = {
     "dns4096": dict(N=4096, Re=1.0e5, K0=4.0, CFL=0.1, UPDATE=100, ADAPT_VISC=0, seed=0, steps=500, warmup=100),
+    "dns16384": dict(N=16384, Re=1.0e6, K0=5.0, CFL=0.2, UPDATE=10, ADAPT_VISC=0, seed=0, steps=31, warmup=10),
     "dns29400": dict(N=29400, Re=1.0e7, K0=4.0, CFL=0.1, UPDATE=20, ADAPT_VISC=0, seed=0, steps=21, warmup=20),
 }
 WORKLOAD = dict(WORKLOADS["dns4096"])
@@ -65,8 +67,9 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="FP64 oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["dns4096", "dns29400", "ensemble"], default="dns4096",
-                    help="dns29400: N=29400 (44100^2 grid, the reference README's large run); "
+    ap.add_argument("--workload", choices=["dns4096", "dns16384", "dns29400", "ensemble"], default="dns4096",
+                    help="dns16384 / dns29400: N=16384 (24576^2 grid) / N=29400 (44100^2 grid), the "
+                         "reference's recorded and README large runs; "
                          "ensemble: the 64-member batched configuration (32xN=128, 24xN=256, 8xN=512)")
     a = ap.parse_args()
     select_workload(a.workload, a.n)
@@ -75,9 +78,9 @@ def parse():
         a.steps = WORKLOAD["steps"]
     if a.warmup is None:
         a.warmup = WORKLOAD["warmup"]
-    if a.workload == "dns29400":
-        # the FP64 oracle needs > 100 GB of host memory here, and a host round trip of the
-        # 7 GB state per step would dominate the e2e figure: both are reported at N=4096
+    if a.workload in ("dns16384", "dns29400"):
+        # the FP64 oracle needs tens of GB of host memory here, and a host round trip of the
+        # multi-GB state per step would dominate the e2e figure: both are reported at N=4096
         a.no_cpu_baseline = True
         a.no_e2e = True
     return a
@@ -363,9 +366,9 @@ def main_ours(args):
         line["e2e"] = r["e2e"]
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
-    elif args.workload == "dns29400":
+    elif args.workload in ("dns16384", "dns29400"):
         line["cpu_baseline"] = None
-        line["cpu_baseline_note"] = "FP64 oracle needs > 100 GB host memory at N=29400; see the N=4096 line"
+        line["cpu_baseline_note"] = f"FP64 oracle needs tens of GB of host memory at N={args.n}; see the N=4096 line"
     print(json.dumps(line), flush=True)
 
 

@@ -241,12 +241,15 @@ const KernelSet *kernel_set(int N)
         Launch<16>::make(),   Launch<32>::make(),   Launch<64>::make(),
         Launch<128>::make(),  Launch<256>::make(),  Launch<512>::make(),
         Launch<1024>::make(), Launch<2048>::make(), Launch<4096>::make(),
-        LaunchC<840>::make(), LaunchC<29400>::make(),
+        LaunchC<840>::make(), LaunchC<16384>::make(), LaunchC<29400>::make(),
     };
     for (const KernelSet &k : sets)
         if (k.N == N) return &k;
     return nullptr;
 }
+
+// sizes served by the 4-CTA cluster kernels (one configuration each: not autotuned)
+bool cluster_size(int N) { return N == 840 || N == 16384 || N == 29400; }
 
 // ============================================================================================
 // small non-templated kernels
@@ -2142,7 +2145,7 @@ extern "C" int dns2d_batch_autotune(dns2d_batch *b)
         return ms / (float)reps;
     };
     for (BatchGroup &g : b->groups) {
-        if (g.N == 840 || g.N == 29400) continue;
+        if (cluster_size(g.N)) continue;
         const int reps = g.N >= 2048 ? 10 : 50;
         Tuning best = g.tune;
         float tb = 1e30f;
@@ -2414,7 +2417,7 @@ extern "C" int dns2d_autotune(int N, int device, int *config)
     const KernelSet *ks = kernel_set(N);
     if (!ks) return DNS2D_ERR_SIZE;
     Tuning best;
-    if (N != 840 && N != 29400) {  // the cluster sizes have a single configuration
+    if (!cluster_size(N)) {  // the cluster sizes have a single configuration
         t_in_autotune = true;
         dns2d_state *s = nullptr;
         int rc = dns2d_create(&s, N, 1.0e5f, 4.0f, 0.1f, device);

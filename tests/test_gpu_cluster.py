@@ -1,8 +1,9 @@
 """The cluster path (every row / column transform of L = 4 M points spread over 4 CTAs with
-distributed shared memory), used where a row exceeds one CTA's shared memory (N = 29400,
-L = 44100).  N = 840 (L = 1260 = 4 x 315) runs the same kernels at a size the FP64 oracle checks
-with the tolerances of the single-CTA path; N = 29400 is checked through size-independent
-properties (energy history against the state, energy decay, restart round trip of U, W)."""
+distributed shared memory), used where a row exceeds one CTA's shared memory (N = 16384,
+L = 24576; N = 29400, L = 44100).  N = 840 (L = 1260 = 4 x 315) runs the same kernels at a size
+the FP64 oracle checks with the tolerances of the single-CTA path; the large sizes are checked
+through one-dimensional transforms against numpy, size-independent properties (energy history
+against the state, energy decay, restart round trip of U, W) and the reference's own results."""
 import os
 import subprocess
 
@@ -183,7 +184,7 @@ def _k2(N):
     return kx * kx + kz * kz
 
 
-@pytest.mark.parametrize("N", [NC, 29400])
+@pytest.mark.parametrize("N", [NC, 16384, 29400])
 def test_cluster_nonlinear_term_of_sparse_field(N):
     """FN of a 7-mode field against its direct convolution: on the 47 modes FN occupies,
     within 2e-6 of max |FN|; elsewhere only FP32 transform rounding, which FN weights by up to
@@ -215,8 +216,9 @@ def _band(om, n):
 
 
 @pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference harness not built")
-def test_cluster_n29400_matches_fp64_and_reference_cufft(tmp_path):
-    """N = 29400 (44100^2 padded grid), seeded k^4 field, 3 steps, against
+@pytest.mark.parametrize("N,Re", [(16384, 1e6), (29400, 1e7)])
+def test_cluster_large_n_matches_fp64_and_reference_cufft(N, Re, tmp_path):
+    """N = 16384 / 29400 (24576^2 / 44100^2 padded grids), seeded k^4 field, 3 steps, against
     - the FP64 oracle: the field is band-limited (its float32 modes vanish beyond |k| ~ 30), so
       3 steps of it are resolved exactly by the oracle at N' = 512 run with the same dt / cn
       sequence; vorticity on |k| < 256 within 2e-7 relative L2;
@@ -224,7 +226,7 @@ def test_cluster_n29400_matches_fp64_and_reference_cufft(tmp_path):
       whole field within 1e-4.  FN multiplies each code's FP32 transform rounding by K^2 (up to
       2e8 here), so modes where the field is ~0 fill with independent FP32 noise in either code;
       the FP64 comparison above is the accuracy statement."""
-    N, Re, K0, cfl, steps, NB = 29400, 1e7, 4.0, 0.1, 3, 512
+    K0, cfl, steps, NB = 4.0, 0.1, 3, 512
     om0 = P().k4_spectrum(N, K0, 11)
     f = tmp_path / "om2.bin"
     om0.tofile(f)
@@ -257,3 +259,43 @@ def test_cluster_n29400_matches_fp64_and_reference_cufft(tmp_path):
     assert err_ours <= 2e-7, (err_ours, err_ref, change)
     assert np.max(np.abs(E / E_ref - 1)) <= 1e-6
     assert _chunked_rel_l2(om, om_ref) <= 1e-4
+
+
+@pytest.mark.parametrize("N", [NC, 4096, 16384, 29400])
+def test_one_dimensional_transforms_match_numpy(N):
+    """OM2PHYS of a field on the kx = 0 column is one length-L inverse transform along z, the same
+    in every column of the plane; of a field on the kz = 0 row, one along x, the same in every row.
+    Against numpy in FP64: relative L2 <= 2e-6 (FP32 transforms of up to 44100 = 2^2 3^2 5^2 7^2
+    points)."""
+    H, L = N // 2, 3 * N // 2
+    rng = np.random.default_rng(N)
+    kz = np.where(np.arange(N) < H, np.arange(N), np.arange(N) - N)
+    s = P().Solver(N, 1e4, 4.0, 0.1)
+    # kx = 0 column, Hermitian in kz (real field); no mean, no kz = -N/2 (its partner is not kept)
+    c = (rng.standard_normal(H) + 1j * rng.standard_normal(H)) / (1.0 + np.arange(H)) ** 0.5
+    c[0] = 0.0
+    col = np.zeros(N, dtype=np.complex128)
+    col[:H] = c
+    col[N - H + 1:] = np.conj(c[1:][::-1])
+    om = np.zeros((N, H), dtype=np.complex64)
+    om[:, 0] = col
+    s.init_vorticity(om)
+    s.om2phys()
+    w = s.phys(2)
+    full = np.zeros(L, dtype=np.complex128)
+    full[kz % L] = om[:, 0]
+    f = (np.fft.ifft(full) * L).real
+    for x in sorted({0, 1, L // 3, L // 2, L - 1, int(rng.integers(L))}):
+        assert rel_l2(w[:, x].astype(np.float64), f) < 2e-6
+    del w
+    # kz = 0 row
+    r = (rng.standard_normal(H) + 1j * rng.standard_normal(H)) / (1.0 + np.arange(H)) ** 0.5
+    r[0] = 0.0
+    om = np.zeros((N, H), dtype=np.complex64)
+    om[0, :] = r
+    s.init_vorticity(om)
+    s.om2phys()
+    w = s.phys(2)
+    g = np.fft.irfft(om[0, :].astype(np.complex128), n=L) * L
+    for z in sorted({0, 1, L // 3, L // 2, L - 1, int(rng.integers(L))}):
+        assert rel_l2(w[z, :].astype(np.float64), g) < 2e-6

@@ -82,38 +82,43 @@ def test_twenty_steps_match_oracle(N):
     assert rel_l2(fg[big], fr[big]) <= 1e-5
 
 
-def test_pao_start_matches_reference_stdout(golden):
-    """The reference's own N=512 run: PAO stats, init CFLM, it=1 and it=100 lines."""
-    run = [r for r in golden["runs"] if r["file"].startswith("sim_output_512")][0]
+@pytest.mark.parametrize("name", ["sim_output_512_1001", "sim_output_4096_501", "sim_output_16384_21",
+                                  "sim_output_16384_101"])
+def test_pao_start_matches_reference_stdout(golden, name):
+    """The reference's own recorded runs (N = 512, 4096 and 16384, PAO-k^-3 start): PAO seed and
+    energy, the initial CFLM, then T, DT, CN, CFLM and SIG at every printed iteration (the first
+    1000 steps of the N = 512 run).  Up to step 100: the printed digits, one float ulp of CN and
+    3e-7 relative on CFLM.  Later the two FP32 trajectories (the recording GPU's cuFFT and this
+    code) drift apart: CFLM within 2e-5, CN within 5e-6, T within 1e-6 relative, SIG within 1."""
+    run = [r for r in golden["runs"] if r["file"].startswith(name + "_")][0]
     s = P().Solver(run["N"], run["Re"], run["K0"], run["CFL"])
     stats, seed = s.init_pao()
     assert seed == run["pao_seed"]
     assert stats[1] == pytest.approx(float(run["pao"]["Energy"]), abs=2e-7)
     cflm = s.next_dt()
     assert cflm == pytest.approx(run["nextdt_init"]["CFLM"], rel=3e-7)
-    its = {r["it"]: r for r in run["iterations"]}
-    s.step(1)
-    s.next_dt()
-    s.om2phys()
-    sig = s.display_sigma(2)
-    sc = s.scalars()
-    g = its[1]
-    assert sc["t"] == pytest.approx(g["T"], abs=2e-10)
-    # CN is printed with 8 decimals; FP32 rounding of CFLM moves it by up to one float ulp (6e-8)
-    assert sc["cn"] == pytest.approx(g["CN"], abs=1.2e-7)
-    assert sc["cflm"] == pytest.approx(g["CFLM"], rel=3e-7)
-    assert int(sig) == g["SIG"]
-    s.step(99)
-    s.next_dt()
-    s.om2phys()
-    sig = s.display_sigma(2)
-    sc = s.scalars()
-    g = its[100]
-    assert sc["t"] == pytest.approx(g["T"], abs=2e-10)
-    assert sc["dt"] == pytest.approx(g["DT"], abs=1e-8)
-    assert sc["cn"] == pytest.approx(g["CN"], abs=1.2e-7)
-    assert sc["cflm"] == pytest.approx(g["CFLM"], rel=1e-6)
-    assert int(sig) == g["SIG"]
+    done = 0
+    for g in run["iterations"]:
+        if g["it"] > 1000:
+            break
+        s.step(g["it"] - done)
+        done = g["it"]
+        s.next_dt()
+        s.om2phys()
+        sig = s.display_sigma(2)
+        sc = s.scalars()
+        assert sc["dt"] == pytest.approx(g["DT"], abs=1e-8), g["it"]
+        if g["it"] <= 100:
+            assert sc["t"] == pytest.approx(g["T"], abs=2e-10), g["it"]
+            # CN is printed with 8 decimals; FP32 rounding of CFLM moves it by up to one float ulp
+            assert sc["cn"] == pytest.approx(g["CN"], abs=1.2e-7), g["it"]
+            assert sc["cflm"] == pytest.approx(g["CFLM"], rel=3e-7 if g["it"] < 100 else 1e-6), g["it"]
+            assert int(sig) == g["SIG"], g["it"]
+        else:
+            assert sc["t"] == pytest.approx(g["T"], rel=1e-6), g["it"]
+            assert sc["cn"] == pytest.approx(g["CN"], abs=5e-6), g["it"]
+            assert sc["cflm"] == pytest.approx(g["CFLM"], rel=2e-5), g["it"]
+            assert abs(int(sig) - g["SIG"]) <= 1, g["it"]
 
 
 def test_omega_phys_and_sigma_match_oracle():
