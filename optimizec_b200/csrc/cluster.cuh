@@ -51,6 +51,8 @@ struct CfgC {
 // the register allocator
 //           N      NT  MINB  local radix plan (product = 3N/8)
 DNS2D_CFGC(840,    63,  1,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
+DNS2D_CFGC(8192,  256,  2,  16, 16, 12)  // L = 12288 = 4 x 3072
+DNS2D_CFGC(9216,  288,  2,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
 DNS2D_CFGC(16384, 384,  2,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
 DNS2D_CFGC(29400, 525,  1,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
 #undef DNS2D_CFGC

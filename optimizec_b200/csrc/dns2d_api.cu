@@ -241,7 +241,8 @@ const KernelSet *kernel_set(int N)
         Launch<16>::make(),   Launch<32>::make(),   Launch<64>::make(),
         Launch<128>::make(),  Launch<256>::make(),  Launch<512>::make(),
         Launch<1024>::make(), Launch<2048>::make(), Launch<4096>::make(),
-        LaunchC<840>::make(), LaunchC<16384>::make(), LaunchC<29400>::make(),
+        LaunchC<840>::make(),  LaunchC<8192>::make(), LaunchC<9216>::make(),
+        LaunchC<16384>::make(), LaunchC<29400>::make(),
     };
     for (const KernelSet &k : sets)
         if (k.N == N) return &k;
@@ -249,7 +250,7 @@ const KernelSet *kernel_set(int N)
 }
 
 // sizes served by the 4-CTA cluster kernels (one configuration each: not autotuned)
-bool cluster_size(int N) { return N == 840 || N == 16384 || N == 29400; }
+bool cluster_size(int N) { return N == 840 || N == 8192 || N == 9216 || N == 16384 || N == 29400; }
 
 // ============================================================================================
 // small non-templated kernels

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_supported_sizes_and_errors():
     L = P.lib()
-    for n in (16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 840, 16384, 29400):
+    for n in (16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 840, 8192, 9216, 16384, 29400):
         assert L.dns2d_supported(n) == 1
     for n in (0, 7, 100, 4095):
         assert L.dns2d_supported(n) == 0

@@ -184,7 +184,7 @@ def _k2(N):
     return kx * kx + kz * kz
 
 
-@pytest.mark.parametrize("N", [NC, 16384, 29400])
+@pytest.mark.parametrize("N", [NC, 8192, 9216, 16384, 29400])
 def test_cluster_nonlinear_term_of_sparse_field(N):
     """FN of a 7-mode field against its direct convolution: on the 47 modes FN occupies,
     within 2e-6 of max |FN|; elsewhere only FP32 transform rounding, which FN weights by up to
@@ -261,7 +261,7 @@ def test_cluster_large_n_matches_fp64_and_reference_cufft(N, Re, tmp_path):
     assert _chunked_rel_l2(om, om_ref) <= 1e-4
 
 
-@pytest.mark.parametrize("N", [NC, 4096, 16384, 29400])
+@pytest.mark.parametrize("N", [NC, 4096, 8192, 9216, 16384, 29400])
 def test_one_dimensional_transforms_match_numpy(N):
     """OM2PHYS of a field on the kx = 0 column is one length-L inverse transform along z, the same
     in every column of the plane; of a field on the kz = 0 row, one along x, the same in every row.
