@@ -51,8 +51,8 @@ struct CfgC {
 // the register allocator
 //           N      NT  MINB  local radix plan (product = 3N/8)
 DNS2D_CFGC(840,    63,  1,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
-DNS2D_CFGC(8192,  256,  2,  16, 16, 12)  // L = 12288 = 4 x 3072
-DNS2D_CFGC(9216,  288,  2,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
+DNS2D_CFGC(8192,  256,  3,  16, 16, 12)  // L = 12288 = 4 x 3072
+DNS2D_CFGC(9216,  288,  3,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
 DNS2D_CFGC(16384, 384,  2,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
 DNS2D_CFGC(29400, 525,  1,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
 #undef DNS2D_CFGC
@@ -80,6 +80,18 @@ __device__ __forceinline__ float2 cross_tw(const float2 *__restrict__ tw, int r,
     constexpr int OFF = TwCatC<N>::off(4, CfgC<N>::M);
     static_assert(OFF >= 0, "cross stage missing from the catalog");
     return __ldg(tw + OFF + (size_t)(r - 1) * CfgC<N>::M + m);
+}
+
+// Cluster barrier without release / acquire ordering.  Used where the barrier only has to hold
+// every CTA of the cluster (all started before distributed shared memory is written; none gone
+// while a peer still reads its shared memory), and nothing written before it is read across the
+// cluster after it.  A full cl.sync() there would also wait for this thread's outstanding global
+// stores.  Remote values read before it are already consumed (they feed the stores issued before
+// the barrier), so those reads are complete.
+__device__ __forceinline__ void cluster_sync_relaxed()
+{
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
 }
 
 // the 4 CTAs' copies of a shared-memory array
@@ -152,7 +164,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         const int k = 4 * k2 + c;
         if (k >= H && k <= L - H) s[sidx(k2)] = make_float2(0.f, 0.f);
     }
-    cl.sync();
+    cluster_sync_relaxed();
     {
         constexpr int HQ = (H + 3) / 4;
         const int k0 = c * HQ, k1 = min(H, k0 + HQ);
@@ -196,7 +208,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
             Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
         }
     }
-    cl.sync();
+    cluster_sync_relaxed();
 }
 
 // kz index kzi = 4 k2 + c of this CTA -> compact iz (-1: the 3/2 padding band)
@@ -275,6 +287,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     float2 *sD = s, *sE = s + MP;
     const Peers pD(cl, sD), pE(cl, sE);
     const int m0 = c * MQ, m1 = min(M, (c + 1) * MQ);
+    cluster_sync_relaxed();  // every CTA of the cluster running before its shared memory is written
     for (int m = m0 + threadIdx.x; m < m1; m += NT) {
         float2 d[4], e[4];
 #pragma unroll
@@ -354,7 +367,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 #pragma unroll
         for (int q = 0; q < 4; ++q) p.work[widx<L, H>(1, m + q * M, kx)] = x[q];
     }
-    cl.sync();
+    cluster_sync_relaxed();
 }
 
 // ------------------------------------------------------------------------------------------
@@ -472,6 +485,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     const int c = (int)cl.block_rank();
     const int z = blockIdx.x >> 2;
     const Peers pe(cl, s);
+    cluster_sync_relaxed();  // every CTA of the cluster running before its shared memory is written
     for (int m = c * MQ + threadIdx.x; m < min(M, (c + 1) * MQ); m += NT) {
         float2 x[4];
 #pragma unroll
