@@ -1970,6 +1970,11 @@ struct dns2d_batch {
     double2 *hist_host = nullptr;    // pinned, count * kChunk entries
     float *cflm_host = nullptr;      // pinned, count entries
     cudaEvent_t prm_copied = nullptr;
+    // one capture stream per size group: the groups' step chains are independent, so a chunk's
+    // graph holds them as parallel branches (forked from and joined back into `stream`)
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork = nullptr;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     bool initialised = false;
     std::string err;
@@ -2016,6 +2021,11 @@ extern "C" void dns2d_batch_destroy(dns2d_batch *b)
     if (b->hist_host) cudaFreeHost(b->hist_host);
     if (b->cflm_host) cudaFreeHost(b->cflm_host);
     if (b->prm_copied) cudaEventDestroy(b->prm_copied);
+    for (cudaStream_t q : b->side)
+        if (q) cudaStreamDestroy(q);
+    for (cudaEvent_t e : b->joins)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -2086,6 +2096,15 @@ extern "C" int dns2d_batch_create(dns2d_batch **out, const dns2d_member *members
         cudaMallocHost((void **)&b->hist_host, (size_t)count * kChunk * 16) != cudaSuccess ||
         cudaMallocHost((void **)&b->cflm_host, (size_t)count * 4) != cudaSuccess)
         return bail(DNS2D_ERR_NOMEM);
+    if (b->groups.size() > 1) {
+        if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
+        b->side.assign(b->groups.size(), nullptr);
+        b->joins.assign(b->groups.size(), nullptr);
+        for (size_t i = 0; i < b->groups.size(); ++i)
+            if (cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming) != cudaSuccess)
+                return bail(DNS2D_ERR_CUDA);
+    }
     *out = b;
     return DNS2D_OK;
 }
@@ -2277,11 +2296,21 @@ extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, doub
         } else {
             cudaGraph_t gr = nullptr;
             BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            for (int i = 0; i < K; ++i)
-                for (BatchGroup &g : b->groups) {
-                    g.ks->rows_step(g.ptrs(), b->stream, g.count);
-                    g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, b->stream, g.count);
+            const bool par = !b->side.empty();
+            if (par) BATCH_CUDA(cudaEventRecord(b->fork, b->stream), "fork");
+            for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+                BatchGroup &g = b->groups[gi];
+                cudaStream_t q = par ? b->side[gi] : b->stream;
+                if (par) BATCH_CUDA(cudaStreamWaitEvent(q, b->fork, 0), "fork wait");
+                for (int i = 0; i < K; ++i) {
+                    g.ks->rows_step(g.ptrs(), q, g.count);
+                    g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, q, g.count);
                 }
+                if (par) {
+                    BATCH_CUDA(cudaEventRecord(b->joins[gi], q), "join");
+                    BATCH_CUDA(cudaStreamWaitEvent(b->stream, b->joins[gi], 0), "join wait");
+                }
+            }
             BATCH_CUDA(cudaStreamEndCapture(b->stream, &gr), "end capture");
             cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
             cudaGraphDestroy(gr);
