@@ -339,13 +339,22 @@ class Solver:
             setattr(s, k, v)
         self._chk(self._L.dns2d_set_scalars(self._s, C.byref(s)))
 
-    def om2(self) -> np.ndarray:
-        out = np.zeros((self.N, self.H), dtype=np.complex64)
+    def _spectrum_out(self, out):
+        if out is None:
+            return np.zeros((self.N, self.H), dtype=np.complex64)
+        if out.dtype != np.complex64 or out.shape != (self.N, self.H) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous complex64 array of shape ({self.N}, {self.H})")
+        return out
+
+    def om2(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Vorticity [iz][ix] (N x N/2 complex64); `out` (e.g. a view of pinned memory) is filled
+        in place when given."""
+        out = self._spectrum_out(out)
         self._chk(self._L.dns2d_get_om2(self._s, _fp(out.view(np.float32))))
         return out
 
-    def fnm1(self) -> np.ndarray:
-        out = np.zeros((self.N, self.H), dtype=np.complex64)
+    def fnm1(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = self._spectrum_out(out)
         self._chk(self._L.dns2d_get_fnm1(self._s, _fp(out.view(np.float32))))
         return out
 
