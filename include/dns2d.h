@@ -228,15 +228,19 @@ int dns2d_closure_tensor_cores(dns2d_state *s, int enable);
 int dns2d_closure_clamp(dns2d_state *s, float alpha);
 
 /* Autotuner (no counterpart in the reference): times the kernel variants of size N on a scratch
- * state on `device` -- rows per CTA of the small-grid row pass, one or two thread groups per
- * column CTA and the L2 prefetch distances of the large-grid passes -- and keeps the fastest for
- * states and batches created afterwards on that device.  All variants compute the same
- * arithmetic, so results do not depend on the choice.  config (nullable) receives
- * {rows_tile, cols_groups, pf_rows, pf_cols} (0 = the size's default).  DNS2D_AUTOTUNE=1 in the
- * environment makes dns2d_create tune its size once per process. */
+ * state on `device` -- rows per CTA and the radix plans of the small-grid (N <= 512) row and
+ * column passes, one or two thread groups per column CTA and the L2 prefetch distances of the
+ * large-grid passes -- and keeps the fastest for states and batches created afterwards on that
+ * device.  Rows per CTA, thread groups and prefetch distances do not change the arithmetic; a
+ * radix plan changes the FP32 rounding (every plan meets the oracle tolerances), and an
+ * alternative plan is kept only when it is at least 3 % faster than the default one.  config
+ * (nullable, 6 ints) receives {rows_tile, cols_groups, pf_rows, pf_cols, plan_rows, plan_cols}
+ * (0 = the size's default).  DNS2D_AUTOTUNE=1 in the environment makes dns2d_create tune its
+ * size once per process. */
 int dns2d_autotune(int N, int device, int *config);
-/* Pin a configuration {rows_tile (0, 2, 4, 8), cols_groups (0, 1, 2), pf_rows, pf_cols} for size
- * N on `device` (no counterpart in the reference); used by states created afterwards. */
+/* Pin a configuration {rows_tile (0, 2, 4, 8), cols_groups (0, 1, 2), pf_rows, pf_cols,
+ * plan_rows, plan_cols (0 .. plans of N - 1; 3 plans at N = 64 ... 512, else 1)} for size N on
+ * `device` (no counterpart in the reference); used by states created afterwards. */
 int dns2d_set_tuning(int N, int device, const int *config);
 
 /* ---- phase timing: PHASE_TIMING of cuda/dns_cuda.cu:26-150 on the fused kernels ---- */

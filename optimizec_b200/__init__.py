@@ -191,16 +191,17 @@ def supported(N: int) -> bool:
 
 def autotune(N: int, device: int = 0) -> dict:
     """Time the kernel variants of size N and keep the fastest (dns2d_autotune)."""
-    cfg = (C.c_int * 4)()
+    cfg = (C.c_int * 6)()
     rc = lib().dns2d_autotune(N, device, cfg)
     if rc:
         raise Dns2dError(f"dns2d_autotune: {lib().dns2d_strerror(rc).decode()}")
-    return dict(zip(("rows_tile", "cols_groups", "pf_rows", "pf_cols"), list(cfg)))
+    return dict(zip(("rows_tile", "cols_groups", "pf_rows", "pf_cols", "plan_rows", "plan_cols"), list(cfg)))
 
 
-def set_tuning(N: int, rows_tile=0, cols_groups=0, pf_rows=296, pf_cols=74, device: int = 0):
+def set_tuning(N: int, rows_tile=0, cols_groups=0, pf_rows=296, pf_cols=74, plan_rows=0, plan_cols=0,
+               device: int = 0):
     """Pin the kernel configuration of size N (dns2d_set_tuning)."""
-    cfg = (C.c_int * 4)(rows_tile, cols_groups, pf_rows, pf_cols)
+    cfg = (C.c_int * 6)(rows_tile, cols_groups, pf_rows, pf_cols, plan_rows, plan_cols)
     rc = lib().dns2d_set_tuning(N, device, cfg)
     if rc:
         raise Dns2dError(f"dns2d_set_tuning: {lib().dns2d_strerror(rc).decode()}")

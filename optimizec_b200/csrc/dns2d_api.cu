@@ -42,6 +42,7 @@ namespace {
 
 struct KernelSet {
     int N;
+    int nplans;  // radix plans of the small-grid passes (AltPlans<N>::count)
     int rows_blocks;
     const TwCatalog *cat;
     cudaError_t (*setup)();
@@ -66,6 +67,33 @@ struct Launch {
 
     static constexpr bool V2 = Cfg2<N>::enabled;
     static constexpr size_t sm2 = V2 ? (size_t)SmemLen<3 * N / 2>::value * sizeof(float2) : 0;
+    using P0 = typename C::Plan;
+    using P1 = typename AltPlans<N>::P1;
+    using P2 = typename AltPlans<N>::P2;
+
+    template <class Plan>
+    static cudaError_t setup_plan()
+    {
+        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_rows_step<N, 2, Plan>, a, (int)(2 * C::LP * sizeof(float2)))) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(k_rows_step<N, 4, Plan>, a, (int)(4 * C::LP * sizeof(float2)))) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(k_rows_step<N, 8, Plan>, a, (int)(8 * C::LP * sizeof(float2)))) != cudaSuccess)
+            return e;
+        return cudaFuncSetAttribute(k_cols_step<N, Plan>, a, (int)smA);
+    }
+    // rows per CTA (autotuned): 2, 4 or 8; the arithmetic per row is the same
+    template <class Plan>
+    static void rows_plan(const Pointers &p, cudaStream_t s, int ny)
+    {
+        const int rt = p.rows_tile ? p.rows_tile : C::ROWS;
+        const size_t sm = (size_t)rt * C::LP * sizeof(float2);
+        if (rt == 2) k_rows_step<N, 2, Plan><<<dim3(C::L / 2, ny), C::NTB, sm, s>>>(p);
+        else if (rt == 8) k_rows_step<N, 8, Plan><<<dim3(C::L / 8, ny), C::NTB, sm, s>>>(p);
+        else k_rows_step<N, 4, Plan><<<dim3(C::L / 4, ny), C::NTB, sm, s>>>(p);
+    }
 
     static cudaError_t setup()
     {
@@ -76,13 +104,10 @@ struct Launch {
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
         }
-        if constexpr (!V2) {  // the rows-per-CTA variants of the small-grid row pass
-            if ((e = cudaFuncSetAttribute(k_rows_step<N, 2>, a, (int)(2 * C::LP * sizeof(float2)))) != cudaSuccess)
-                return e;
-            if ((e = cudaFuncSetAttribute(k_rows_step<N, 4>, a, (int)(4 * C::LP * sizeof(float2)))) != cudaSuccess)
-                return e;
-            if ((e = cudaFuncSetAttribute(k_rows_step<N, 8>, a, (int)(8 * C::LP * sizeof(float2)))) != cudaSuccess)
-                return e;
+        if constexpr (!V2) {  // rows per CTA x radix plan variants of the small-grid passes
+            if ((e = setup_plan<P0>()) != cudaSuccess) return e;
+            if ((e = setup_plan<P1>()) != cudaSuccess) return e;
+            if ((e = setup_plan<P2>()) != cudaSuccess) return e;
         }
         if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_init<N>, a, (int)smA)) != cudaSuccess) return e;
@@ -99,12 +124,9 @@ struct Launch {
         if constexpr (V2) {
             k_rows_step2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p);
         } else {
-            // rows per CTA (autotuned): 2, 4 or 8; the arithmetic per row is the same
-            const int rt = p.rows_tile ? p.rows_tile : C::ROWS;
-            const size_t sm = (size_t)rt * C::LP * sizeof(float2);
-            if (rt == 2) k_rows_step<N, 2><<<dim3(C::L / 2, ny), C::NTB, sm, s>>>(p);
-            else if (rt == 8) k_rows_step<N, 8><<<dim3(C::L / 8, ny), C::NTB, sm, s>>>(p);
-            else k_rows_step<N, 4><<<dim3(C::L / 4, ny), C::NTB, sm, s>>>(p);
+            if (p.plan_rows == 1) rows_plan<P1>(p, s, ny);
+            else if (p.plan_rows == 2) rows_plan<P2>(p, s, ny);
+            else rows_plan<P0>(p, s, ny);
         }
     }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
@@ -116,7 +138,9 @@ struct Launch {
             if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
             else k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         }
-        else k_cols_step<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
+        else if (p.plan_cols == 1) k_cols_step<N, P1><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
+        else if (p.plan_cols == 2) k_cols_step<N, P2><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
+        else k_cols_step<N, P0><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
     }
     static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
     {
@@ -148,7 +172,8 @@ struct Launch {
     }
     static KernelSet make()
     {
-        return KernelSet{N, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
+        return KernelSet{N, AltPlans<N>::count, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init,
+                         rows_velocity,
                          rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar};
     }
 };
@@ -205,7 +230,7 @@ struct LaunchC {
     }
     static KernelSet make()
     {
-        return KernelSet{N, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
+        return KernelSet{N, 1, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
                          rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr};
     }
 };
@@ -214,6 +239,7 @@ struct LaunchC {
 // so the choice changes speed only
 struct Tuning {
     int rows_tile = 0, cols_groups = 0, pf_rows = 296, pf_cols = 74;
+    int plan_rows = 0, plan_cols = 0;  // radix plans (these change the rounding)
 };
 
 std::mutex g_tune_mu;
@@ -233,6 +259,41 @@ void apply_tuning(Pointers &p, const Tuning &t)
     p.cols_groups = t.cols_groups;
     p.pf_rows = t.pf_rows;
     p.pf_cols = t.pf_cols;
+    p.plan_rows = t.plan_rows;
+    p.plan_cols = t.plan_cols;
+}
+
+// Small-grid tuning: rows per CTA x radix plan for the row pass, radix plan for the column pass.
+// time(t, rows) returns the time of one pass under configuration t.  An alternative plan (which
+// rounds differently) replaces plan 0 only when it is at least 3 % faster.
+template <class F>
+Tuning tune_small(int nplans, Tuning best, F time)
+{
+    float t0 = 1e30f, tb = 1e30f;
+    Tuning b0 = best, bb = best;
+    for (int pl = 0; pl < nplans; ++pl)
+        for (int rt : {2, 4, 8}) {
+            Tuning t = best;
+            t.plan_rows = pl;
+            t.rows_tile = rt;
+            const float ms = time(t, true);
+            if (pl == 0 && ms < t0) t0 = ms, b0.rows_tile = rt, b0.plan_rows = 0;
+            if (ms < tb) tb = ms, bb.rows_tile = rt, bb.plan_rows = pl;
+        }
+    if (bb.plan_rows != 0 && tb > 0.97f * t0) bb = b0;
+    best.rows_tile = bb.rows_tile;
+    best.plan_rows = bb.plan_rows;
+    t0 = tb = 1e30f;
+    int pb = 0;
+    for (int pl = 0; pl < nplans; ++pl) {
+        Tuning t = best;
+        t.plan_cols = pl;
+        const float ms = time(t, false);
+        if (pl == 0) t0 = ms;
+        if (ms < tb) tb = ms, pb = pl;
+    }
+    best.plan_cols = (pb != 0 && tb > 0.97f * t0) ? 0 : pb;
+    return best;
 }
 
 const KernelSet *kernel_set(int N)
@@ -2188,13 +2249,12 @@ extern "C" int dns2d_batch_autotune(dns2d_batch *b)
                     if (t < tb) tb = t, best.cols_groups = gr, best.pf_cols = pf;
                 }
         } else {
-            for (int rt : {2, 4, 8}) {
-                g.tune = best;
-                g.tune.rows_tile = rt;
+            best = tune_small(g.ks->nplans, best, [&](const Tuning &t, bool rows) {
+                g.tune = t;
                 const Pointers p = g.ptrs();
-                const float t = timed([&] { g.ks->rows_step(p, b->stream, g.count); }, reps);
-                if (t < tb) tb = t, best.rows_tile = rt;
-            }
+                if (rows) return timed([&] { g.ks->rows_step(p, b->stream, g.count); }, reps);
+                return timed([&] { g.ks->cols_step(p, 0, 0, b->stream, g.count); }, reps);
+            });
         }
         g.tune = best;
     }
@@ -2428,15 +2488,19 @@ float time_launches(dns2d_state *s, int reps, F fn)
 
 extern "C" int dns2d_set_tuning(int N, int device, const int *config)
 {
-    if (!kernel_set(N) || !config) return DNS2D_ERR_ARG;
+    const KernelSet *ks = kernel_set(N);
+    if (!ks || !config) return DNS2D_ERR_ARG;
     if (!(config[0] == 0 || config[0] == 2 || config[0] == 4 || config[0] == 8) || config[1] < 0 || config[1] > 2 ||
-        config[2] < 0 || config[3] < 0)
+        config[2] < 0 || config[3] < 0 || config[4] < 0 || config[4] >= ks->nplans || config[5] < 0 ||
+        config[5] >= ks->nplans)
         return DNS2D_ERR_ARG;
     Tuning t;
     t.rows_tile = config[0];
     t.cols_groups = config[1];
     t.pf_rows = config[2];
     t.pf_cols = config[3];
+    t.plan_rows = config[4];
+    t.plan_cols = config[5];
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[{device, N}] = t;
     return DNS2D_OK;
@@ -2482,13 +2546,12 @@ extern "C" int dns2d_autotune(int N, int device, int *config)
                     if (t < tb) tb = t, best.cols_groups = g, best.pf_cols = pf;
                 }
         } else {
-            for (int rt : {2, 4, 8}) {
-                s->tune = best;
-                s->tune.rows_tile = rt;
+            best = tune_small(ks->nplans, best, [&](const Tuning &t, bool rows) {
+                s->tune = t;
                 const Pointers p = s->ptrs();
-                const float t = time_launches(s, reps, [&] { ks->rows_step(p, s->stream, 1); });
-                if (t < tb) tb = t, best.rows_tile = rt;
-            }
+                if (rows) return time_launches(s, reps, [&] { ks->rows_step(p, s->stream, 1); });
+                return time_launches(s, reps, [&] { ks->cols_step(p, 0, 0, s->stream, 1); });
+            });
         }
         const cudaError_t e = cudaStreamSynchronize(s->stream);
         dns2d_destroy(s);
@@ -2503,6 +2566,8 @@ extern "C" int dns2d_autotune(int N, int device, int *config)
         config[1] = best.cols_groups;
         config[2] = best.pf_rows;
         config[3] = best.pf_cols;
+        config[4] = best.plan_rows;
+        config[5] = best.plan_cols;
     }
     return DNS2D_OK;
 }

@@ -54,8 +54,9 @@ def test_ensemble_configuration():
 
 
 def test_batch_autotune_keeps_results():
-    """dns2d_batch_autotune (before init) picks kernel variants with the same arithmetic: the
-    tuned batch reproduces the untuned one bit for bit."""
+    """dns2d_batch_autotune (before init) picks kernel variants per size group: the tuned batch
+    reproduces the untuned one bit for bit where the group keeps its default radix plans, and to
+    FP32 rounding (relative L2 <= 1e-6 after 10 steps) where the tuner picked another plan."""
     import optimizec_b200 as P
     ms = [(128, 3e3, 3.0, 0.1, 1), (256, 1e4, 4.0, 0.1, 2), (128, 1e4, 5.0, 0.1, 3), (1024, 1e4, 4.0, 0.1, 4)]
     out = []
@@ -71,4 +72,5 @@ def test_batch_autotune_keeps_results():
         out.append([b.om2(m) for m in range(len(ms))])
         b.close()
     for a, c in zip(out[0], out[1]):
-        np.testing.assert_array_equal(a, c)
+        a, c = a.astype(np.complex128), c.astype(np.complex128)
+        assert np.linalg.norm(a - c) / np.linalg.norm(a) <= 1e-6
