@@ -47,6 +47,9 @@ SYMBOLS = [
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# translation units of libdns2d.so: the C ABI and one unit per group of compiled grid sizes
+SOURCES = ["dns2d_api.cu", "sets_small.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
+           "sets_29400.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]
 
@@ -72,11 +75,23 @@ class Member(C.Structure):
 
 def build(verbose: bool = False) -> str:
     """Compile libdns2d.so (sm_100a) and the mem_cuda CLI in-tree."""
-    src = os.path.join(_HERE, "csrc", "dns2d_api.cu")
-    cmd = [NVCC, *ARCH, *CUFLAGS, "-Xcompiler", "-fPIC", "-shared", "-o", LIB_PATH, src]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.check_call(cmd)
+    import tempfile
+    with tempfile.TemporaryDirectory(prefix="dns2d_build_") as tmp:
+        objs, procs = [], []
+        for src in SOURCES:  # one nvcc per translation unit, in parallel
+            obj = os.path.join(tmp, src.replace(".cu", ".o"))
+            cmd = [NVCC, *ARCH, *CUFLAGS, "-Xcompiler", "-fPIC", "-c", "-o", obj, os.path.join(_HERE, "csrc", src)]
+            if verbose:
+                print(" ".join(cmd))
+            objs.append(obj)
+            procs.append((cmd, subprocess.Popen(cmd)))
+        failed = [cmd for cmd, pr in procs if pr.wait() != 0]
+        if failed:
+            raise subprocess.CalledProcessError(1, failed[0])
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB_PATH, *objs]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
     cli_src = os.path.join(_HERE, "cli", "mem_cuda.cpp")
     if os.path.exists(cli_src):
         cli = os.path.join(_HERE, "mem_cuda")

@@ -7,8 +7,7 @@
 // cuda/step3_cuda.cu:172), so printed T/DT/CN values follow the reference.  The device sees
 // dt/cn/cnm1 through a small parameter block written by a one-thread kernel at the start of
 // every dns2d_step call, which lets one captured graph serve every segment.
-#include "dns2d_kernels.cuh"
-#include "cluster.cuh"
+#include "kernel_sets.cuh"
 #include "cnn.cuh"
 #include "cnn_tc.cuh"
 #include "../../include/dns2d.h"
@@ -36,204 +35,9 @@
 using namespace dns2d;
 
 // ============================================================================================
-// kernel sets, one per compiled N
+// kernel configuration and the table of compiled sizes (kernel_sets.cuh, sets_*.cu)
 // ============================================================================================
 namespace {
-
-struct KernelSet {
-    int N;
-    int nplans;  // radix plans of the small-grid passes (AltPlans<N>::count)
-    int rows_blocks;
-    const TwCatalog *cat;
-    cudaError_t (*setup)();
-    void (*rows_step)(const Pointers &, cudaStream_t, int);
-    void (*cols_step)(const Pointers &, int, int, cudaStream_t, int);
-    void (*cols_init)(const Pointers &, const float2 *, int, cudaStream_t, int);
-    void (*rows_velocity)(const Pointers &, float *, float *, float, cudaStream_t, int);
-    void (*rows_from_phys)(const Pointers &, const float *, cudaStream_t);
-    void (*cols_scalar)(const Pointers &, float2 *, int, cudaStream_t);
-    void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
-    void (*rows_fwd_scalar)(const Pointers &, const float *, float2 *, cudaStream_t);
-    void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, cudaStream_t);
-};
-
-template <int N>
-struct Launch {
-    using C = Cfg<N>;
-    static constexpr size_t smB = (size_t)C::ROWS * C::LP * sizeof(float2);
-    static constexpr size_t smA = (size_t)2 * C::LP * sizeof(float2);
-    static constexpr size_t smA1 = (size_t)C::LP * sizeof(float2);
-    static constexpr int GB = C::L / C::ROWS;
-
-    static constexpr bool V2 = Cfg2<N>::enabled;
-    static constexpr size_t sm2 = V2 ? (size_t)SmemLen<3 * N / 2>::value * sizeof(float2) : 0;
-    using P0 = typename C::Plan;
-    using P1 = typename AltPlans<N>::P1;
-    using P2 = typename AltPlans<N>::P2;
-
-    template <class Plan>
-    static cudaError_t setup_plan()
-    {
-        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        cudaError_t e;
-        if ((e = cudaFuncSetAttribute(k_rows_step<N, 2, Plan>, a, (int)(2 * C::LP * sizeof(float2)))) != cudaSuccess)
-            return e;
-        if ((e = cudaFuncSetAttribute(k_rows_step<N, 4, Plan>, a, (int)(4 * C::LP * sizeof(float2)))) != cudaSuccess)
-            return e;
-        if ((e = cudaFuncSetAttribute(k_rows_step<N, 8, Plan>, a, (int)(8 * C::LP * sizeof(float2)))) != cudaSuccess)
-            return e;
-        return cudaFuncSetAttribute(k_cols_step<N, Plan>, a, (int)smA);
-    }
-    // rows per CTA (autotuned): 2, 4 or 8; the arithmetic per row is the same
-    template <class Plan>
-    static void rows_plan(const Pointers &p, cudaStream_t s, int ny)
-    {
-        const int rt = p.rows_tile ? p.rows_tile : C::ROWS;
-        const size_t sm = (size_t)rt * C::LP * sizeof(float2);
-        if (rt == 2) k_rows_step<N, 2, Plan><<<dim3(C::L / 2, ny), C::NTB, sm, s>>>(p);
-        else if (rt == 8) k_rows_step<N, 8, Plan><<<dim3(C::L / 8, ny), C::NTB, sm, s>>>(p);
-        else k_rows_step<N, 4, Plan><<<dim3(C::L / 4, ny), C::NTB, sm, s>>>(p);
-    }
-
-    static cudaError_t setup()
-    {
-        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        cudaError_t e;
-        if constexpr (V2) {
-            if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
-            if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
-            if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
-        }
-        if constexpr (!V2) {  // rows per CTA x radix plan variants of the small-grid passes
-            if ((e = setup_plan<P0>()) != cudaSuccess) return e;
-            if ((e = setup_plan<P1>()) != cudaSuccess) return e;
-            if ((e = setup_plan<P2>()) != cudaSuccess) return e;
-        }
-        if ((e = cudaFuncSetAttribute(k_cols_step<N>, a, (int)smA)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_init<N>, a, (int)smA)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_velocity<N>, a, (int)smB)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_from_phys<N>, a, (int)smB)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_fwd_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_fwd_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
-        return cudaSuccess;
-    }
-    static void rows_step(const Pointers &p, cudaStream_t s, int ny)
-    {
-        if constexpr (V2) {
-            k_rows_step2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p);
-        } else {
-            if (p.plan_rows == 1) rows_plan<P1>(p, s, ny);
-            else if (p.plan_rows == 2) rows_plan<P2>(p, s, ny);
-            else rows_plan<P0>(p, s, ny);
-        }
-    }
-    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
-    {
-        // two thread groups per column CTA (autotuned; default from B200 measurements: faster at
-        // N = 4096, slower at 2048); both give the same arithmetic
-        if constexpr (V2) {
-            const int g = p.cols_groups ? p.cols_groups : (N >= 4096 ? 2 : 1);
-            if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
-            else k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
-        }
-        else if (p.plan_cols == 1) k_cols_step<N, P1><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
-        else if (p.plan_cols == 2) k_cols_step<N, P2><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
-        else k_cols_step<N, P0><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
-    }
-    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
-    {
-        k_cols_init<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, uw, mode);
-    }
-    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s, int ny)
-    {
-        k_rows_velocity<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p, phys, cflm, dx);
-    }
-    static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
-    {
-        k_rows_from_phys<N><<<GB, C::NTB, smB, s>>>(p, phys);
-    }
-    static void cols_scalar(const Pointers &p, float2 *scratch, int kind, cudaStream_t s)
-    {
-        k_cols_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, kind);
-    }
-    static void rows_scalar(const Pointers &p, const float2 *scratch, float *out, float2 *mm, cudaStream_t s)
-    {
-        k_rows_scalar<N><<<GB, C::NTB, smB, s>>>(p, scratch, out, mm);
-    }
-    static void rows_fwd_scalar(const Pointers &p, const float *f, float2 *scratch, cudaStream_t s)
-    {
-        k_rows_fwd_scalar<N><<<GB, C::NTB, smB, s>>>(p, f, scratch);
-    }
-    static void cols_fwd_scalar(const Pointers &p, const float2 *scratch, float2 *out, cudaStream_t s)
-    {
-        k_cols_fwd_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, out);
-    }
-    static KernelSet make()
-    {
-        return KernelSet{N, AltPlans<N>::count, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init,
-                         rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar};
-    }
-};
-
-// Sizes whose rows exceed one CTA's shared memory: every transform runs on a cluster of 4 CTAs
-// (cluster.cuh).  Grids are 4 CTAs per row / column; the closure's forward scalar transforms are
-// not provided at these sizes.
-template <int N>
-struct LaunchC {
-    using C = CfgC<N>;
-    static constexpr size_t sm1 = (size_t)C::MP * sizeof(float2);
-    static constexpr size_t sm2 = 2 * sm1;
-
-    static cudaError_t setup()
-    {
-        const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        cudaError_t e;
-        if ((e = cudaFuncSetAttribute(k_rows_step_c<N>, a, (int)sm1)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_step_c<N>, a, (int)sm2)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_init_c<N>, a, (int)sm2)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_velocity_c<N>, a, (int)sm1)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_from_phys_c<N>, a, (int)sm1)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_cols_scalar_c<N>, a, (int)sm1)) != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_rows_scalar_c<N>, a, (int)sm1)) != cudaSuccess) return e;
-        return cudaSuccess;
-    }
-    static void rows_step(const Pointers &p, cudaStream_t s, int ny)
-    {
-        k_rows_step_c<N><<<dim3(4 * C::L, ny), C::NT, sm1, s>>>(p);
-    }
-    static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
-    {
-        k_cols_step_c<N><<<dim3(4 * C::H, ny), C::NT, sm2, s>>>(p, first, slot);
-    }
-    static void cols_init(const Pointers &p, const float2 *uw, int mode, cudaStream_t s, int ny)
-    {
-        k_cols_init_c<N><<<dim3(4 * C::H, ny), C::NT, sm2, s>>>(p, uw, mode);
-    }
-    static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s, int ny)
-    {
-        k_rows_velocity_c<N><<<dim3(4 * C::L, ny), C::NT, sm1, s>>>(p, phys, cflm, dx);
-    }
-    static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
-    {
-        k_rows_from_phys_c<N><<<4 * C::L, C::NT, sm1, s>>>(p, phys);
-    }
-    static void cols_scalar(const Pointers &p, float2 *scratch, int kind, cudaStream_t s)
-    {
-        k_cols_scalar_c<N><<<4 * C::H, C::NT, sm1, s>>>(p, scratch, kind);
-    }
-    static void rows_scalar(const Pointers &p, const float2 *scratch, float *out, float2 *mm, cudaStream_t s)
-    {
-        k_rows_scalar_c<N><<<4 * C::L, C::NT, sm1, s>>>(p, scratch, out, mm);
-    }
-    static KernelSet make()
-    {
-        return KernelSet{N, 1, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr};
-    }
-};
 
 // kernel configuration of one size on one device; every variant computes the same arithmetic,
 // so the choice changes speed only
@@ -298,15 +102,10 @@ Tuning tune_small(int nplans, Tuning best, F time)
 
 const KernelSet *kernel_set(int N)
 {
-    static const KernelSet sets[] = {
-        Launch<16>::make(),   Launch<32>::make(),   Launch<64>::make(),
-        Launch<128>::make(),  Launch<256>::make(),  Launch<512>::make(),
-        Launch<1024>::make(), Launch<2048>::make(), Launch<4096>::make(),
-        LaunchC<840>::make(),  LaunchC<8192>::make(), LaunchC<9216>::make(),
-        LaunchC<16384>::make(), LaunchC<29400>::make(),
-    };
-    for (const KernelSet &k : sets)
-        if (k.N == N) return &k;
+    // one translation unit per group of sizes (sets_*.cu), compiled in parallel
+    for (const KernelSet *(*part)(int) : {kernel_sets_small, kernel_sets_mid, kernel_sets_4096, kernel_sets_cluster,
+                                          kernel_sets_16384, kernel_sets_29400})
+        if (const KernelSet *k = part(N)) return k;
     return nullptr;
 }
 
