@@ -208,3 +208,29 @@ def test_twenty_steps_match_reference_cufft(N, tmp_path):
     err = float(np.linalg.norm(om - om_ref) / np.linalg.norm(om_ref))
     assert err <= 1e-5, err
     assert np.max(np.abs(E / E_ref - 1)) <= 1e-6
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built")
+@pytest.mark.parametrize("args", [[16384, "1E6", 5, 21, 0.2, 10, 0], [2048, "1E5", 4, 200, 0.1, 50, 0]])
+def test_cli_matches_reference_binary(args, tmp_path):
+    """The reference's own command lines (its recorded N=16384 run on the cluster path, and an
+    N=2048 run), both binaries from their PAO start on the same GPU: the PAO seed and every printed
+    iteration line (T, DT, CN, CFLM, SIG) agree to FP32 transform rounding."""
+    (tmp_path / "r").mkdir()
+    (tmp_path / "o").mkdir()
+    env = {"BENCH_WARMUP_STEPS": "0"}
+    ref = run_cli(args, tmp_path / "r", env=env, exe=REF, timeout=900)
+    ours = run_cli(args, tmp_path / "o", env=env, timeout=900)
+    assert ref.returncode == 0, ref.stderr[-2000:]
+    assert ours.returncode == 0, ours.stderr[-2000:]
+    seed = re.compile(r"PAO seed\s*=\s*(\d+)")
+    assert seed.search(ref.stdout)[1] == seed.search(ours.stdout)[1]
+    r, o = iterations(ref.stdout), iterations(ours.stdout)
+    assert sorted(r) == sorted(o) and len(r) >= 3
+    for it in r:
+        # T is printed with 10 decimals: one unit of the last digit is 1e-10
+        assert o[it]["T"] == pytest.approx(r[it]["T"], rel=1e-6, abs=1.5e-10)
+        assert o[it]["DT"] == pytest.approx(r[it]["DT"], rel=1e-5, abs=2e-8)
+        assert o[it]["CN"] == pytest.approx(r[it]["CN"], abs=2e-6)
+        assert o[it]["CFLM"] == pytest.approx(r[it]["CFLM"], rel=1e-5)
+        assert abs(o[it]["SIG"] - r[it]["SIG"]) <= 1
