@@ -112,7 +112,10 @@ int dns2d_get_fnm1(dns2d_state *s, float *fnm1);
 int dns2d_get_phys(dns2d_state *s, int comp, float *plane);
 /* load u, w physical planes (e.g. a restart file's UR_full) as the current velocity */
 int dns2d_set_velocity_phys(dns2d_state *s, const float *u, const float *w);
-/* restart.bin v2 writer / v1+v2 reader (cuda/mem_cuda.cu:1019-1394 byte layout) */
+/* restart.bin v2 writer / v1+v2 reader (cuda/mem_cuda.cu:1019-1394 byte layout).  The file moves
+ * through three pinned staging buffers of up to 64 MiB each (allocated at the first save or load,
+ * freed by dns2d_destroy), with device<->host copies overlapping the file writes / reads.  A load
+ * checks the header and the file size before it touches the state. */
 int dns2d_save_restart(dns2d_state *s, const char *path);
 int dns2d_load_restart(dns2d_state *s, const char *path);
 
