@@ -2030,7 +2030,7 @@ extern "C" int dns2d_batch_autotune(dns2d_batch *b)
         Tuning best = g.tune;
         float tb = 1e30f;
         if (g.N >= 1024) {
-            for (int pf : {0, 148, 296, 592}) {
+            for (int pf : {0, 148, 296, 444, 592}) {
                 g.tune = best;
                 g.tune.pf_rows = pf;
                 const Pointers p = g.ptrs();
@@ -2327,7 +2327,7 @@ extern "C" int dns2d_autotune(int N, int device, int *config)
         const bool large = N >= 1024;
         float tb = 1e30f;
         if (large) {
-            for (int pf : {0, 148, 296, 592}) {
+            for (int pf : {0, 148, 296, 444, 592}) {
                 s->tune = best;
                 s->tune.pf_rows = pf;
                 const Pointers p = s->ptrs();

@@ -457,8 +457,10 @@ struct TwCat {
     static constexpr int off(int R, int NS) { return cat.find(R, NS); }
 };
 
+// three CTAs per SM: the register allocator keeps the row pass at 56 registers (36 warps per SM;
+// N = 4096: 0.311 -> 0.280 ms against two CTAs at 80 registers)
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_rows_step2(Pointers p0)
+__global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
