@@ -37,24 +37,25 @@ struct CfgC {
     static constexpr bool enabled = false;
 };
 
-#define DNS2D_CFGC(N_, NT_, MINB_, ...)                                                        \
+#define DNS2D_CFGC(N_, NT_, MINBR_, MINBC_, ...)                                               \
     template <>                                                                                \
     struct CfgC<N_> {                                                                          \
         static constexpr bool enabled = true;                                                  \
         static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, M = L / 4;                    \
-        static constexpr int MP = SmemLen<M>::value, NT = NT_, MINB = MINB_;                   \
+        static constexpr int MP = SmemLen<M>::value, NT = NT_, MINB_R = MINBR_, MINB_C = MINBC_; \
         static constexpr int MQ = (M + 3) / 4; /* butterflies of the cluster radix per CTA */ \
         using Plan = Radices<__VA_ARGS__>;                                                     \
         static_assert(L % 4 == 0 && radix_product(Plan{}) == M, "plan");                       \
     };
-// NT threads per CTA (at least M / R for every radix R of the plan); MINB CTAs per SM asked of
-// the register allocator
-//           N      NT  MINB  local radix plan (product = 3N/8)
-DNS2D_CFGC(840,    63,  1,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
-DNS2D_CFGC(8192,  256,  3,  16, 16, 12)  // L = 12288 = 4 x 3072
-DNS2D_CFGC(9216,  288,  3,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
-DNS2D_CFGC(16384, 384,  2,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
-DNS2D_CFGC(29400, 525,  1,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
+// NT threads per CTA (at least M / R for every radix R of the plan); CTAs per SM asked of the
+// register allocator for the row kernels (MINB_R) and the column kernels (MINB_C, two arrays of
+// shared memory and more live values), each the faster of the candidates measured on B200
+//           N      NT  MINB_R MINB_C  local radix plan (product = 3N/8)
+DNS2D_CFGC(840,    63,  1, 1,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
+DNS2D_CFGC(8192,  256,  4, 3,  16, 16, 12)  // L = 12288 = 4 x 3072
+DNS2D_CFGC(9216,  288,  4, 3,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
+DNS2D_CFGC(16384, 384,  3, 2,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
+DNS2D_CFGC(29400, 525,  1, 1,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
 #undef DNS2D_CFGC
 
 template <int N>
@@ -143,7 +144,7 @@ __device__ __forceinline__ float2 packed_uw(const float2 *__restrict__ U, const 
 // Row pass: U, W row z -> C2R -> (u + iw)^2 -> R2C -> D, E row z.  Grid (4 L, members).
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB) k_rows_step_c(Pointers p0)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_R) k_rows_step_c(Pointers p0)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = CfgC<N>;
@@ -270,7 +271,7 @@ __device__ __forceinline__ void cluster_energy(cg::cluster_group &cl, const Poin
 // 3/2 padding -> z-inverse -> U, W column kx.  Grid (4 H, members).
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_C)
     k_cols_step_c(Pointers p0, int first, int hist_slot)
 {
     const Pointers p = p0.member(blockIdx.y);
@@ -375,7 +376,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 // i (kz u - kx w), fnm1 = 0), mode 1 velocity recovery from om2.  -> U, W columns.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_C)
     k_cols_init_c(Pointers p0, const float2 *__restrict__ uw, int mode)
 {
     const Pointers p = p0.member(blockIdx.y);
@@ -430,7 +431,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 // and CFL maximum.
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_R)
     k_rows_velocity_c(Pointers p0, float *phys, float *cflm, float dx)
 {
     const Pointers p = p0.member(blockIdx.y);
@@ -474,7 +475,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 // Physical rows -> U, W rows (k_rows_from_phys semantics, x-forward of u + iw scaled by 1/L).
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_R)
     k_rows_from_phys_c(Pointers p, const float *phys)
 {
     using C = CfgC<N>;
@@ -516,7 +517,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 // Scalar field to physical space (k_cols_scalar / k_rows_scalar semantics).
 // ------------------------------------------------------------------------------------------
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_C)
     k_cols_scalar_c(Pointers p, float2 *scratch, int kind)
 {
     using C = CfgC<N>;
@@ -554,7 +555,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
 }
 
 template <int N>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB)
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>::MINB_R)
     k_rows_scalar_c(Pointers p, const float2 *scratch, float *out, float2 *minmax)
 {
     using C = CfgC<N>;
