@@ -420,18 +420,20 @@ struct Cfg2 {
     static constexpr bool enabled = false;
 };
 
-#define DNS2D_CFG2(N_, NT_, R1_, R2_, R3_)                                                     \
+#define DNS2D_CFG2(N_, NT_, R1_, R2_, R3_, MC2_, MC4_)                                         \
     template <>                                                                                \
     struct Cfg2<N_> {                                                                          \
         static constexpr bool enabled = true;                                                  \
         static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, LP = SmemLen<L>::value;       \
         static constexpr int NT = NT_, R1 = R1_, R2 = R2_, R3 = R3_;                           \
+        static constexpr int MC2 = MC2_, MC4 = MC4_; /* CTAs per SM: k_cols_step2, k_cols_step4 */ \
         static_assert(R1_ * R2_ * R3_ == L, "plan");                                           \
         static_assert(L / R1_ <= NT_ && L / R2_ <= NT_ && L / R3_ <= NT_, "one butterfly");    \
     };
-DNS2D_CFG2(1024, 192, 16, 8, 12)
-DNS2D_CFG2(2048, 256, 16, 16, 12)
-DNS2D_CFG2(4096, 384, 16, 16, 24)
+//          N    NT  plan (R1, R2, R3)  column CTAs per SM asked of the register allocator
+DNS2D_CFG2(1024, 192, 16, 8, 12,       2, 1)
+DNS2D_CFG2(2048, 256, 16, 16, 12,      2, 2)  // two-group columns at 64 registers, 2 CTAs per SM
+DNS2D_CFG2(4096, 384, 16, 16, 24,      2, 1)
 #undef DNS2D_CFG2
 
 // twiddle catalog of size N: the stages of every plan compiled for it
@@ -564,7 +566,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
 }
 
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 2) k_cols_step2(Pointers p0, int first, int hist_slot)
+__global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointers p0, int first, int hist_slot)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
@@ -758,7 +760,7 @@ __device__ __forceinline__ void stage1g_last_band(float2 *s, const float2 *tw, i
 }
 
 template <int N>
-__global__ void __launch_bounds__(2 * Cfg2<N>::NT, 1) k_cols_step4(Pointers p0, int first, int hist_slot)
+__global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Pointers p0, int first, int hist_slot)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;

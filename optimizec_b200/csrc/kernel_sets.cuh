@@ -99,10 +99,10 @@ struct Launch {
     }
     static void cols_step(const Pointers &p, int first, int slot, cudaStream_t s, int ny)
     {
-        // two thread groups per column CTA (autotuned; default from B200 measurements: faster at
-        // N = 4096, slower at 2048); both give the same arithmetic
+        // one or two thread groups per column CTA (autotuned; the default, two, was the faster on
+        // B200 at N = 1024, 2048 and 4096); both give the same arithmetic
         if constexpr (V2) {
-            const int g = p.cols_groups ? p.cols_groups : (N >= 4096 ? 2 : 1);
+            const int g = p.cols_groups ? p.cols_groups : 2;
             if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
             else k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         }
