@@ -48,7 +48,7 @@ SYMBOLS = [
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # translation units of libdns2d.so: the C ABI and one unit per group of compiled grid sizes
-SOURCES = ["dns2d_api.cu", "sets_small.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
+SOURCES = ["dns2d_api.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
            "sets_29400.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]

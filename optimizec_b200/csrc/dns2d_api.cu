@@ -103,8 +103,8 @@ Tuning tune_small(int nplans, Tuning best, F time)
 const KernelSet *kernel_set(int N)
 {
     // one translation unit per group of sizes (sets_*.cu), compiled in parallel
-    for (const KernelSet *(*part)(int) : {kernel_sets_small, kernel_sets_mid, kernel_sets_4096, kernel_sets_cluster,
-                                          kernel_sets_16384, kernel_sets_29400})
+    for (const KernelSet *(*part)(int) : {kernel_sets_small, kernel_sets_256, kernel_sets_mid, kernel_sets_4096,
+                                          kernel_sets_cluster, kernel_sets_16384, kernel_sets_29400})
         if (const KernelSet *k = part(N)) return k;
     return nullptr;
 }

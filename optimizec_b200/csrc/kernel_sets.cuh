@@ -205,7 +205,8 @@ struct LaunchC {
 
 
 // the compiled sizes, by translation unit (nullptr: N is not in that unit)
-const KernelSet *kernel_sets_small(int N);    // 16 ... 512 (sets_small.cu)
+const KernelSet *kernel_sets_small(int N);    // 16 ... 128 (sets_small.cu)
+const KernelSet *kernel_sets_256(int N);      // 256, 512 (sets_256.cu)
 const KernelSet *kernel_sets_mid(int N);      // 1024, 2048 (sets_mid.cu)
 const KernelSet *kernel_sets_4096(int N);     // 4096 (sets_4096.cu)
 const KernelSet *kernel_sets_cluster(int N);  // 840, 8192, 9216 (sets_cluster.cu)

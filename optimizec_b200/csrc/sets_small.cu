@@ -1,4 +1,4 @@
-// sets_small.cu — kernel sets of the small single-CTA sizes (N = 16 ... 512).
+// sets_small.cu — kernel sets of the small single-CTA sizes (N = 16 ... 128).
 #include "kernel_sets.cuh"
 
 namespace dns2d {
@@ -10,8 +10,6 @@ const KernelSet *kernel_sets_small(int N)
         Launch<32>::make(),
         Launch<64>::make(),
         Launch<128>::make(),
-        Launch<256>::make(),
-        Launch<512>::make(),
     };
     for (const KernelSet &k : sets)
         if (k.N == N) return &k;
