@@ -2156,21 +2156,24 @@ extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, doub
             cudaGraph_t gr = nullptr;
             BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             const bool par = !b->side.empty();
-            if (par) BATCH_CUDA(cudaEventRecord(b->fork, b->stream), "fork");
-            for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+            // a failure inside the capture still ends it (the stream leaves capture mode)
+            cudaError_t ce = par ? cudaEventRecord(b->fork, b->stream) : cudaSuccess;
+            for (size_t gi = 0; gi < b->groups.size() && ce == cudaSuccess; ++gi) {
                 BatchGroup &g = b->groups[gi];
                 cudaStream_t q = par ? b->side[gi] : b->stream;
-                if (par) BATCH_CUDA(cudaStreamWaitEvent(q, b->fork, 0), "fork wait");
-                for (int i = 0; i < K; ++i) {
+                if (par) ce = cudaStreamWaitEvent(q, b->fork, 0);
+                for (int i = 0; i < K && ce == cudaSuccess; ++i) {
                     g.ks->rows_step(g.ptrs(), q, g.count);
                     g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, q, g.count);
                 }
-                if (par) {
-                    BATCH_CUDA(cudaEventRecord(b->joins[gi], q), "join");
-                    BATCH_CUDA(cudaStreamWaitEvent(b->stream, b->joins[gi], 0), "join wait");
-                }
+                if (par && ce == cudaSuccess) ce = cudaEventRecord(b->joins[gi], q);
+                if (par && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->joins[gi], 0);
             }
-            BATCH_CUDA(cudaStreamEndCapture(b->stream, &gr), "end capture");
+            const cudaError_t ee = cudaStreamEndCapture(b->stream, &gr);
+            if (ce != cudaSuccess || ee != cudaSuccess) {
+                if (gr) cudaGraphDestroy(gr);
+                return bfail(b, DNS2D_ERR_CUDA, "graph capture", ce != cudaSuccess ? ce : ee);
+            }
             cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
             cudaGraphDestroy(gr);
             if (e != cudaSuccess) return bfail(b, DNS2D_ERR_CUDA, "graph instantiate", e);
