@@ -471,6 +471,10 @@ if __name__ == "__main__":
     a = parse()
     if a.workload == "ensemble" and a.impl == "ours":
         main_ensemble(a)
+    elif a.workload == "ensemble":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble: each "
+                              "member would be its own mem_cuda process"}), flush=True)
     elif a.impl == "reference":
         main_reference(a)
     else:
