@@ -79,6 +79,10 @@ int dns2d_k4_spectrum(int N, float K0, uint64_t seed, float *om2);
 int dns2d_step(dns2d_state *s, int nsteps, double *E_hist, double *Z_hist);
 /* NEXTDT of cuda/dns_cuda.cu:553-580 on the current velocity; writes CFLM (nullable) */
 int dns2d_next_dt(dns2d_state *s, float *cflm);
+/* Build the CUDA graphs dns2d_step(s, nsteps) will launch, without running them (no counterpart
+ * in the reference): keeps the one-time graph capture out of a timed dns2d_step.  Nothing to do
+ * with a closure attached. */
+int dns2d_prepare(dns2d_state *s, int nsteps);
 /* the state's CUDA stream (a cudaStream_t), for callers that order their own work after it */
 void *dns2d_stream(dns2d_state *s);
 /* wait for the state's stream; watchdog: DNS2D_ERR_TIMEOUT after timeout_ms (<= 0: none) */

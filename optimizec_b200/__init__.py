@@ -43,7 +43,7 @@ SYMBOLS = [
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
-    "dns2d_movie_scale", "dns2d_movie_frame",
+    "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -181,6 +181,7 @@ def lib():
         "dns2d_closure_clamp": (C.c_int, [vp, C.c_float]),
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "dns2d_movie_scale": (C.c_int, [C.c_int]),
+        "dns2d_prepare": (C.c_int, [vp, C.c_int]),
         "dns2d_movie_frame": (C.c_int, [vp, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_double)]),
     }
@@ -288,6 +289,10 @@ class Solver:
             return E, Z
         self._chk(self._L.dns2d_step(self._s, n, None, None))
         return None
+
+    def prepare(self, n: int):
+        """Build the CUDA graphs step(n) will launch, without running them (dns2d_prepare)."""
+        self._chk(self._L.dns2d_prepare(self._s, int(n)))
 
     def next_dt(self) -> float:
         c = C.c_float(0)

@@ -149,3 +149,22 @@ def test_restart_roundtrip(tmp_path):
     s.step(5)
     s2.step(5)
     assert rel_l2(s2.om2().astype(np.complex128), s.om2().astype(np.complex128)) < 1e-6
+
+
+def test_prepare_builds_graphs_without_stepping():
+    """dns2d_prepare captures the graphs of a later dns2d_step without running them: the state
+    does not move, and the prepared run equals an unprepared one bit for bit."""
+    N = 256
+    a = P().Solver(N, 1e4, 4.0, 0.1)
+    b = P().Solver(N, 1e4, 4.0, 0.1)
+    for s in (a, b):
+        s.init_k4(4)
+        s.next_dt()
+    om0 = a.om2()
+    a.prepare(200)
+    a.sync()
+    assert a.scalars()["it"] == 0
+    np.testing.assert_array_equal(a.om2(), om0)
+    a.step(200)
+    b.step(200)
+    np.testing.assert_array_equal(a.om2(), b.om2())
