@@ -178,6 +178,8 @@ int dns2d_batch_init_k4(dns2d_batch *b);
 int dns2d_batch_next_dt(dns2d_batch *b, float *cflm);
 /* nsteps steps of every member; E_hist / Z_hist (nullable) are [count][nsteps] */
 int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, double *Z_hist);
+/* build the graphs a later dns2d_batch_step(b, nsteps) launches, without running them */
+int dns2d_batch_prepare(dns2d_batch *b, int nsteps);
 int dns2d_batch_sync(dns2d_batch *b);
 int dns2d_batch_get_om2(dns2d_batch *b, int member, float *om2);
 int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars *out);

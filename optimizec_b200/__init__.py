@@ -43,7 +43,7 @@ SYMBOLS = [
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
-    "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare",
+    "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare", "dns2d_batch_prepare",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -182,6 +182,7 @@ def lib():
         "dns2d_closure_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "dns2d_movie_scale": (C.c_int, [C.c_int]),
         "dns2d_prepare": (C.c_int, [vp, C.c_int]),
+        "dns2d_batch_prepare": (C.c_int, [vp, C.c_int]),
         "dns2d_movie_frame": (C.c_int, [vp, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_double)]),
     }
@@ -473,6 +474,10 @@ class Batch:
     def autotune(self):
         """Time each size group's kernel variants at its member count (before init_k4)."""
         self._chk(self._L.dns2d_batch_autotune(self._b))
+
+    def prepare(self, n: int):
+        """Build the graphs step(n) will launch, without running them (dns2d_batch_prepare)."""
+        self._chk(self._L.dns2d_batch_prepare(self._b, int(n)))
 
     def init_k4(self):
         self._chk(self._L.dns2d_batch_init_k4(self._b))

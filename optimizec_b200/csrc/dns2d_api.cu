@@ -2142,6 +2142,63 @@ extern "C" int dns2d_batch_next_dt(dns2d_batch *b, float *cflm_out)
     return DNS2D_OK;
 }
 
+namespace {
+
+// the instantiated graph of a chunk of K steps (first: the chunk opens a dns2d_batch_step call),
+// captured on first use: every size group's step chain as its own branch
+int batch_graph(dns2d_batch *b, int first, int K, cudaGraphExec_t *out)
+{
+    const auto key = std::make_pair(first, K);
+    const auto itg = b->graphs.find(key);
+    if (itg != b->graphs.end()) {
+        *out = itg->second;
+        return DNS2D_OK;
+    }
+    cudaGraph_t gr = nullptr;
+    BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const bool par = !b->side.empty();
+    // a failure inside the capture still ends it (the stream leaves capture mode)
+    cudaError_t ce = par ? cudaEventRecord(b->fork, b->stream) : cudaSuccess;
+    for (size_t gi = 0; gi < b->groups.size() && ce == cudaSuccess; ++gi) {
+        BatchGroup &g = b->groups[gi];
+        cudaStream_t q = par ? b->side[gi] : b->stream;
+        if (par) ce = cudaStreamWaitEvent(q, b->fork, 0);
+        for (int i = 0; i < K && ce == cudaSuccess; ++i) {
+            g.ks->rows_step(g.ptrs(), q, g.count);
+            g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, q, g.count);
+        }
+        if (par && ce == cudaSuccess) ce = cudaEventRecord(b->joins[gi], q);
+        if (par && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->joins[gi], 0);
+    }
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &gr);
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        return bfail(b, DNS2D_ERR_CUDA, "graph capture", ce != cudaSuccess ? ce : ee);
+    }
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return bfail(b, DNS2D_ERR_CUDA, "graph instantiate", e);
+    b->graphs[key] = ex;
+    *out = ex;
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int dns2d_batch_prepare(dns2d_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return DNS2D_ERR_ARG;
+    for (int done = 0; done < nsteps;) {
+        const int K = std::min(kChunk, nsteps - done);
+        cudaGraphExec_t ex = nullptr;
+        const int rc = batch_graph(b, done == 0 ? 1 : 0, K, &ex);
+        if (rc) return rc;
+        done += K;
+    }
+    return DNS2D_OK;
+}
+
 extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, double *Z_hist)
 {
     if (!b || nsteps < 0) return DNS2D_ERR_ARG;
@@ -2164,38 +2221,9 @@ extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, doub
     while (done < nsteps) {
         const int K = std::min(kChunk, nsteps - done);
         const int first = (done == 0) ? 1 : 0;
-        auto key = std::make_pair(first, K);
-        auto itg = b->graphs.find(key);
         cudaGraphExec_t ex = nullptr;
-        if (itg != b->graphs.end()) {
-            ex = itg->second;
-        } else {
-            cudaGraph_t gr = nullptr;
-            BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            const bool par = !b->side.empty();
-            // a failure inside the capture still ends it (the stream leaves capture mode)
-            cudaError_t ce = par ? cudaEventRecord(b->fork, b->stream) : cudaSuccess;
-            for (size_t gi = 0; gi < b->groups.size() && ce == cudaSuccess; ++gi) {
-                BatchGroup &g = b->groups[gi];
-                cudaStream_t q = par ? b->side[gi] : b->stream;
-                if (par) ce = cudaStreamWaitEvent(q, b->fork, 0);
-                for (int i = 0; i < K && ce == cudaSuccess; ++i) {
-                    g.ks->rows_step(g.ptrs(), q, g.count);
-                    g.ks->cols_step(g.ptrs(), (first && i == 0) ? 1 : 0, i, q, g.count);
-                }
-                if (par && ce == cudaSuccess) ce = cudaEventRecord(b->joins[gi], q);
-                if (par && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->joins[gi], 0);
-            }
-            const cudaError_t ee = cudaStreamEndCapture(b->stream, &gr);
-            if (ce != cudaSuccess || ee != cudaSuccess) {
-                if (gr) cudaGraphDestroy(gr);
-                return bfail(b, DNS2D_ERR_CUDA, "graph capture", ce != cudaSuccess ? ce : ee);
-            }
-            cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
-            cudaGraphDestroy(gr);
-            if (e != cudaSuccess) return bfail(b, DNS2D_ERR_CUDA, "graph instantiate", e);
-            b->graphs[key] = ex;
-        }
+        const int rc = batch_graph(b, first, K, &ex);
+        if (rc) return rc;
         BATCH_CUDA(cudaGraphLaunch(ex, b->stream), "graph launch");
         if (E_hist || Z_hist) {
             off = 0;
