@@ -217,9 +217,11 @@ int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, floa
  *                   energy input sum w Re(conj(om/K^2) F) exceeds the viscous loss 2 nu Z
  *                   (steps stay in captured CUDA graphs);
  *   energy_check 2  after each step on the host: a step whose energy rose is rolled back and
- *                   redone without the closure (one host sync per step).
- * dns2d_closure_stats counts closed steps and fallbacks.  The network must not be used by
- * another state or trained while attached. */
+ *                   redone without the closure (one host sync per step);
+ *   energy_check 3  as 1, but the forcing of such a step is scaled by 2 nu Z / P (its energy input
+ *                   then equals the viscous loss) instead of dropped.
+ * dns2d_closure_stats counts closed steps and fallbacks (dropped or scaled steps).  The network
+ * must not be used by another state or trained while attached. */
 int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *scales4, int energy_check);
 /* The spectral forcing the attached closure adds to FN for the current state, in the compact
  * layout of dns2d_get_fnm1 (N x N/2 complex float, [kz][kx]); a diagnostic, the state is not

@@ -398,7 +398,8 @@ class Solver:
 
     def attach_closure(self, net, scales, energy_check: int = 1):
         """Couple a trained CNN (or None to detach); scales = (s_omega, s_u, s_w, s_out);
-        energy_check 0 off, 1 device-side gate (graph-captured), 2 host rollback."""
+        energy_check 0 off, 1 device-side gate (graph-captured), 2 host rollback, 3 device-side
+        scaling of an energy-raising forcing to the viscous loss."""
         sc = np.ascontiguousarray(scales, dtype=np.float32)
         self._closure_net = net  # keep the network alive while attached
         self._chk(self._L.dns2d_closure_attach(self._s, net.handle if net is not None else None, _fp(sc),

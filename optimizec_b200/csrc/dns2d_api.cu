@@ -2882,7 +2882,9 @@ __global__ void k_scale_copy(const float *in, float *out, size_t n, float sc)
 // for this step only when P <= 2 nu Z, otherwise the step runs as the plain coarse step.
 // Grid kGateBlocks x 256: per-block partials, summed in block order by the last block to arrive.
 constexpr int kGateBlocks = 64;
-__global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, float *gate,
+// scale == 0: the forcing is dropped (gate 0) for a step whose energy input P exceeds the viscous
+// loss 2 nu Z; scale == 1: it is scaled by 2 nu Z / P so that its input equals the loss
+__global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, int scale, float *gate,
                                unsigned long long *off, double2 *part, unsigned int *counter)
 {
     __shared__ double sp[256], sz[256];
@@ -2923,8 +2925,9 @@ __global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, fl
             Zs += q.y;
         }
         *counter = 0u;
-        const bool keep = Ps <= 2.0 * (double)visc * Zs;
-        *gate = keep ? 1.0f : 0.0f;
+        const double loss = 2.0 * (double)visc * Zs;
+        const bool keep = Ps <= loss;  // P > loss >= 0 below: the ratio is in [0, 1)
+        *gate = keep ? 1.0f : (scale ? (float)(loss / Ps) : 0.0f);
         if (!keep) *off += 1ULL;
     }
 }
@@ -2977,9 +2980,9 @@ static int closure_device_step(dns2d_state *s, int first, int slot)
     Pointers p = s->ptrs();
     p.force = s->force;
     p.force_clamp = s->closure_clamp;
-    if (s->closure_check == 1) {
-        k_closure_gate<<<kGateBlocks, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->gate, s->gate_off,
-                                                          s->gate_part, s->gate_counter);
+    if (s->closure_check == 1 || s->closure_check == 3) {
+        k_closure_gate<<<kGateBlocks, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->closure_check == 3 ? 1 : 0,
+                                                          s->gate, s->gate_off, s->gate_part, s->gate_counter);
         p.gate = s->gate;
     }
     s->ks->rows_step(p, s->stream, 1);
@@ -3136,7 +3139,7 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
     s->cnn = n;
     for (int c = 0; c < 3; ++c) s->in_scale[c] = scales4[c];
     s->out_scale = scales4[3];
-    s->closure_check = (energy_check < 0 || energy_check > 2) ? 1 : energy_check;
+    s->closure_check = (energy_check < 0 || energy_check > 3) ? 1 : energy_check;
     s->closure_E = -1.0;
     s->closure_steps = 0;
     s->closure_fallbacks = 0;

@@ -148,6 +148,32 @@ def test_energy_gate_drops_anti_dissipative_forcing(pkg, check):
         x.close()
 
 
+def test_energy_scaling_caps_the_forcing_input(pkg):
+    """energy_check 3 with the anti-dissipative F = omega: every step is limited (scaled, not
+    dropped), so the run differs from the plain one, and the forcing's input only replaces the
+    viscous loss: the energy drifts by less than 5 % of the plain run's viscous decay (the time
+    stepping's own O(dt^2) error), where an unlimited F = omega makes it grow."""
+    steps = 40
+    s_p = _state(pkg)
+    s_p.velocity_phys()
+    s_p.om2phys()
+    s_om = float(np.abs(s_p.phys(2)).max()) * 2.0
+    net = _identity_net(pkg, s_om)
+    sc = np.array([s_om, 1.0, 1.0, s_om], dtype=np.float32)
+    E0, _ = s_p.energy_enstrophy()
+    s_s = _state(pkg)
+    s_s.attach_closure(net, sc, energy_check=3)
+    E_p, _ = s_p.step(steps, history=True)
+    E_s, _ = s_s.step(steps, history=True)
+    assert s_s.closure_stats() == (steps, steps)
+    decay = E0 - E_p[-1]
+    assert decay > 0
+    assert np.max(np.abs(E_s - E0)) < 0.05 * decay
+    assert not np.array_equal(s_s.om2(), s_p.om2())
+    for x in (s_p, s_s, net):
+        x.close()
+
+
 def test_trained_closure_improves_coarse_run(pkg):
     """Train on filtered N=256 DNS, run N=32 with and without the closure to the DNS end time."""
     from optimizec_b200 import closure as CL
