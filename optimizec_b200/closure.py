@@ -197,7 +197,11 @@ def main(argv=None):
     ap.add_argument("--train-seconds", type=float, default=420.0)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--clamp", type=float, default=1.0, help="forcing limiter alpha (0: off)")
+    ap.add_argument("--checks", default=None,
+                    help="evaluations as energy_check:alpha pairs, e.g. 1:1,3:1 (default: 1:clamp,1:0,0:0)")
     a = ap.parse_args(argv)
+    runs = ([(int(c), float(al)) for c, al in (x.split(":") for x in a.checks.split(","))] if a.checks
+            else [(1, a.clamp), (1, 0.0), (0, 0.0)])
     cfg = dict(Nf=a.nf, Nc=a.nc, Re=a.re, K0=4.0, cfl=0.1)
     t = time.time()
     X, T = generate(seeds=range(a.seeds), steps=a.steps, every=a.every, warm=a.every, **cfg)
@@ -211,10 +215,11 @@ def main(argv=None):
     print(json.dumps({"train_iters": iters, "train_s": round(time.time() - t, 1),
                       "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-50:]))}),
           flush=True)
-    for chk, clamp in ((1, a.clamp), (1, 0.0), (0, 0.0)):
+    for chk, clamp in runs:
         for fs in (a.steps // 4, a.steps):
             r = evaluate(net, sc, seed=100, fine_steps=fs, update=100, check=chk, clamp=clamp, **cfg)
             r["energy_check"] = chk
+            r["clamp"] = clamp
             r["speedup_closure_vs_dns"] = r["wall_dns"] / r["closure"]["wall"]
             print(json.dumps(r), flush=True)
     net.close()
