@@ -74,3 +74,27 @@ def test_batch_autotune_keeps_results():
     for a, c in zip(out[0], out[1]):
         a, c = a.astype(np.complex128), c.astype(np.complex128)
         assert np.linalg.norm(a - c) / np.linalg.norm(a) <= 1e-6
+
+
+def test_batch_prepare_builds_graphs_without_stepping():
+    """dns2d_batch_prepare captures the chunk graphs of a later dns2d_batch_step without running
+    them: the members do not move, and the prepared batch steps like an unprepared one."""
+    import optimizec_b200 as P
+    ms = [(128, 3e3, 3.0, 0.1, 1), (256, 1e4, 4.0, 0.1, 2)]
+    out = []
+    for prep in (False, True):
+        b = P.Batch(ms)
+        b.init_k4()
+        b.next_dt()
+        before = [b.om2(m) for m in range(len(ms))]
+        if prep:
+            b.prepare(150)
+            b.sync()
+            for m in range(len(ms)):
+                np.testing.assert_array_equal(b.om2(m), before[m])
+                assert b.scalars(m)["it"] == 0
+        b.step(150)
+        out.append([b.om2(m) for m in range(len(ms))])
+        b.close()
+    for a, c in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, c)
