@@ -7,6 +7,13 @@
 // cuda/step3_cuda.cu:172), so printed T/DT/CN values follow the reference.  The device sees
 // dt/cn/cnm1 through a small parameter block written by a one-thread kernel at the start of
 // every dns2d_step call, which lets one captured graph serve every segment.
+//
+// Sections, in order: kernel configuration and tuning; small kernels and FP64 reductions; the
+// state and its life cycle; initial conditions; time stepping; movie frames; diagnostics; state
+// transfer; restart.bin through pinned staging; phase timing; batched ensembles; the closure
+// network, the autotuner and the closure coupling; the time step without device allocation.
+// The kernels of the passes are in dns2d_kernels.cuh / cluster.cuh, their launch tables in
+// kernel_sets.cuh (instantiated by sets_*.cu).
 #include "kernel_sets.cuh"
 #include "cnn.cuh"
 #include "cnn_tc.cuh"
