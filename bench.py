@@ -68,6 +68,12 @@ def parse():
                     help="FP64 oracle steps for cpu_baseline (about 10 s on 16 host cores at N=4096)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile", choices=["step", "closure"], default=None,
+                    help="short run for an ncu capture, nothing timed or printed as a bench line: 'step' = "
+                         "k^4 field (seed 1), NEXTDT, 1 + 3 steps of size --n through the step graphs; "
+                         "'closure' = 3 closed steps at N=256 with a 6 x 32 network")
+    ap.add_argument("--windows", type=int, default=0,
+                    help="number of timed K-step windows (0: as many as fill about 1 s of device time)")
     ap.add_argument("--workload", choices=["dns4096", "dns16384", "dns29400", "ensemble"], default="dns4096",
                     help="dns16384 / dns29400: N=16384 (24576^2 grid) / N=29400 (44100^2 grid), the "
                          "reference's recorded and README large runs; "
@@ -203,6 +209,15 @@ def advance(s, it_to, update, steps_total, counts, history=False):
     return hist
 
 
+def window_plan(W: int, K: int, update: int, ms_per_step_est: float, target_ms: float = 1000.0,
+                max_windows: int = 200):
+    """Start steps of the timed windows: consecutive K-step windows after the W warm-up steps,
+    as many as fill about target_ms of device time (at least 3, at most max_windows)."""
+    n = int(target_ms / max(1e-6, ms_per_step_est * K)) + 1
+    n = max(3, min(max_windows, n))
+    return [W + i * K for i in range(n)]
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -210,20 +225,27 @@ def run_ours(args, rank, world, local_rank):
 
     N, K, W = args.n, args.steps, args.warmup
     up = WORKLOAD["UPDATE"]
-    steps_total = W + K
     torch.cuda.set_device(local_rank)
     tuning = P.autotune(N, local_rank)  # kernel variants with identical arithmetic; fastest kept
     s = P.Solver(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"], device=local_rank)
     s.init_k4(WORKLOAD["seed"] + rank)
     s.next_dt()
-    counts = {"kernels": 0}
-    advance(s, W, up, steps_total, counts)
-    for n in set(segments(W, W + K, up)):  # graph capture stays out of the timed region
-        s.prepare(n)
-    s.sync()
     stream = torch.cuda.ExternalStream(s.stream(), device=local_rank)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    counts = {"kernels": 0}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    advance(s, W, up, W, counts)  # warm-up, ending with a diagnostic step like every window
+    e1.record(stream)
+    s.sync()
+    est = e0.elapsed_time(e1) / max(1, W)
+    starts = window_plan(W, K, up, est) if args.windows <= 0 else [W + i * K for i in range(args.windows)]
+    if world > 1:  # every rank runs the same number of windows
+        starts = starts[:int(-max_over_ranks(-len(starts), world, device=f"cuda:{local_rank}"))]
+    for w0 in starts:  # graph capture stays out of the timed region
+        for n in set(segments(w0, w0 + K, up)):
+            s.prepare(n)
+    s.sync()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in starts]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -231,13 +253,17 @@ def run_ours(args, rank, world, local_rank):
     clocks.start()
     time.sleep(0.3)
     counts = {"kernels": 0}
-    ev0.record(stream)
-    advance(s, W + K, up, steps_total, counts)
-    ev1.record(stream)
+    for (a, b), w0 in zip(evs, starts):
+        a.record(stream)
+        # one window: K steps with the reference's diagnostic cadence, ending on a diagnostic
+        # step as the reference's run ends on it == STEPS
+        advance(s, w0 + K, up, w0 + K, counts)
+        b.record(stream)
     s.sync()
     torch.cuda.synchronize()
     ck = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    win = [a.elapsed_time(b) for a, b in evs]
+    ms = statistics.median(win)
     ms_max = max_over_ranks(ms, world, device=f"cuda:{local_rank}")
     if world > 1:
         torch.distributed.barrier()
@@ -250,52 +276,57 @@ def run_ours(args, rank, world, local_rank):
     s.phase_timing(False)
     rows_ms = ph_ms[0] / max(ph_n[0], 1)
     cols_ms = ph_ms[1] / max(ph_n[1], 1)
+    s.close()
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(s, P, N, K, W, up, local_rank, world)
-    s.close()
+        e2e = run_e2e(P, N, K, W, up, local_rank, world)
     return dict(value=value, ms=ms_max, K=K, W=W, N=N, kernels=counts["kernels"], clocks=ck,
-                rows_ms=rows_ms, cols_ms=cols_ms, e2e=e2e, tuning=tuning)
+                rows_ms=rows_ms, cols_ms=cols_ms, e2e=e2e, tuning=tuning,
+                windows={"count": len(win), "median_ms": round(ms, 4), "min_ms": round(min(win), 4),
+                         "max_ms": round(max(win), 4), "first_ms": round(win[0], 4)})
 
 
-def run_e2e(s_old, P, N, K, W, up, local_rank, world):
-    """Same metric through the public API with host buffers: pinned host state -> device,
-    K steps (per-step FP64 energy/enstrophy back to the host), final state -> host."""
+def run_e2e(P, N, K, W, up, local_rank, world, min_reps: int = 5, target_s: float = 1.0):
+    """Same metric through the public API with host buffers, as a user runs an initial-value
+    problem: the initial vorticity (pinned host memory) -> device, K steps with the per-step FP64
+    energy/enstrophy returned to the host, the final vorticity -> pinned host memory.  Each
+    repetition restarts from the same field; the median repetition is reported."""
     import numpy as np
     import torch
 
     H = N // 2
-    om = P.k4_spectrum(N, WORKLOAD["K0"], WORKLOAD["seed"])
     pin_om = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy()
-    pin_fn = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy()
-    pin_om[...] = om.view(np.float32).reshape(N, H, 2)
-    pin_fn[...] = 0.0
+    pin_om[...] = P.k4_spectrum(N, WORKLOAD["K0"], WORKLOAD["seed"]).view(np.float32).reshape(N, H, 2)
+    om_in = pin_om.view(np.complex64).reshape(N, H)
+    out_om = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy().view(np.complex64).reshape(N, H)
     s = P.Solver(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"], device=local_rank)
-    # warm the graphs of this state
-    s.init_vorticity(pin_om.view(np.complex64).reshape(N, H), pin_fn.view(np.complex64).reshape(N, H))
-    s.next_dt()
-    advance(s, W, up, W + K, {"kernels": 0})
+
+    def one():
+        s.init_vorticity(om_in)  # FNM1 starts at zero on the device, as in a fresh run
+        s.next_dt()
+        advance(s, K, up, K, {"kernels": 0}, history=True)
+        s.om2(out=out_om)  # result into pinned host memory
+
+    one()  # builds the graphs of this state's segment lengths
     for n in set(segments(0, K, up)):
         s.prepare(n)
     s.sync()
-    out_om = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy().view(np.complex64).reshape(N, H)
-    out_fn = torch.empty((N, H, 2), dtype=torch.float32, pin_memory=True).numpy().view(np.complex64).reshape(N, H)
-    if world > 1:
-        torch.distributed.barrier()
-    t0 = time.perf_counter()
-    s.init_vorticity(pin_om.view(np.complex64).reshape(N, H), pin_fn.view(np.complex64).reshape(N, H))
-    s.next_dt()
-    advance(s, K, up, K, {"kernels": 0}, history=True)
-    s.om2(out=out_om)   # results into pinned host buffers
-    s.fnm1(out=out_fn)
-    t1 = time.perf_counter()
-    sec = max_over_ranks(t1 - t0, world, device=f"cuda:{local_rank}")
+    reps = []
+    while len(reps) < min_reps or (sum(reps) < target_s and len(reps) < 100):
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        one()
+        reps.append(time.perf_counter() - t0)
+    sec = max_over_ranks(statistics.median(reps), world, device=f"cuda:{local_rank}")
     s.close()
-    state_bytes = 2 * N * H * 8
+    state_bytes = N * H * 8
     return {"value": world * K / sec, "unit": "steps/s",
-            "h2d_bytes_per_step": (state_bytes + 16 * K) / K,
+            "h2d_bytes_per_step": state_bytes / K,
             "d2h_bytes_per_step": (state_bytes + 16 * K) / K,
-            "what": "pinned host om2+fnm1 -> device, K steps with per-step E/Z to host, om2+fnm1 -> pinned host"}
+            "repetitions": len(reps),
+            "what": "pinned host initial vorticity -> device, K steps with per-step E/Z to host, final vorticity -> "
+                    "pinned host (wall clock, median repetition)"}
 
 
 def cpu_baseline(args):
@@ -365,7 +396,9 @@ def main_ours(args):
         "config": {"workload": workload_text(N) + ", k^4 exp(-2(k/K0)^2) IC",
                    "N": N, "padded_grid": 3 * N // 2, "parallelism": "replicas",
                    "l2": f"inputs larger than L2 (work 12N^2 + state 8N^2 bytes = {20 * N * N / 1e6:.0f} MB)",
-                   "autotuned": r["tuning"]},
+                   "autotuned": r["tuning"],
+                   "timing": "value = K / median device time of consecutive K-step windows (CUDA events on "
+                             "the solver's stream), each window ending on a diagnostic step"},
         "mpts_steps_per_s": round(r["value"] * N * N / 1e6, 1),
         "step_roofline": {"bytes_per_step_survey": 76 * N * N, "bytes_per_step_min": 64 * N * N,
                           "frac_survey": round(76 * N * N * steps_s / (peak * 1e9), 4),
@@ -374,7 +407,9 @@ def main_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": tr, "bytes_per_launch": b, "launch_ms": round(ms, 4)},
         "kernel_ms": {"k_rows_step": round(r["rows_ms"], 4), "k_cols_step": round(r["cols_ms"], 4)},
+        "windows": r["windows"],
         "gpu_launches": r["kernels"],
+        "gpu_launches_note": "kernels of this library launched in all timed windows together",
         "clocks": r["clocks"],
     }
     if r["e2e"]:
@@ -387,44 +422,104 @@ def main_ours(args):
     print(json.dumps(line), flush=True)
 
 
-def main_reference(args):
+def reference_cadence(W: int, K: int, update: int):
+    """(BENCH_WARMUP_STEPS, STEPS) for the reference's mem_cuda so that its "Steady FPS" covers
+    exactly the K steps after a warm-up.  Its steady timer starts only inside a diagnostic step
+    (it == 1, a multiple of UPDATE, or it == STEPS) once it >= BENCH_WARMUP_STEPS
+    (cuda/mem_cuda.cu:1859,1912-1920), so the warm-up is rounded down to the last diagnostic step
+    at or before W: the largest multiple of UPDATE <= W, else step 1."""
+    warm = (W // update) * update if W >= update else 1
+    return warm, warm + K
+
+
+_STEADY = re.compile(r"Steady frames per second \(FPS\)\s*=\s*([0-9.eE+-]+)\s*\((\d+) steps after warmup\)")
+
+
+def parse_reference_stdout(text: str):
+    """(steady steps/s, steps in the steady window) from the reference's end-of-run lines
+    (cuda/mem_cuda.cu:2024-2036), or None when it printed no steady window."""
+    m = _STEADY.search(text)
+    if not m:
+        return None
+    return float(m.group(1)), int(m.group(2))
+
+
+def run_reference_binary(exe: str, argv: list, warm: int, cwd: str, timeout: int = 1800):
+    """One run of the reference CLI; returns (steps/s, steady steps, wall seconds) or raises
+    RuntimeError with the reason and the end of its output."""
+    env = dict(os.environ, BENCH_WARMUP_STEPS=str(warm))
+    t0 = time.perf_counter()
+    p = subprocess.run([exe, *map(str, argv)], env=env, cwd=cwd, capture_output=True, text=True, timeout=timeout)
+    wall = time.perf_counter() - t0
+    r = parse_reference_stdout(p.stdout)
+    if p.returncode != 0 or r is None:
+        why = f"exit code {p.returncode}" if p.returncode != 0 else "no 'Steady frames per second' line"
+        tail = (p.stdout[-300:] + " | " + p.stderr[-200:]).replace("\n", " / ")
+        raise RuntimeError(f"reference mem_cuda {' '.join(map(str, argv))}: {why}; output tail: {tail}")
+    return r[0], r[1], wall
+
+
+def reference_initial_field(N: int, path: str) -> str:
+    """The seeded k^4 exp(-2(k/K0)^2) field of our arm, set up by the FP64 oracle (velocity
+    recovery, C2R, NEXTDT init) and written as restart.bin v2 for the reference's loader."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    o = O.Oracle(N, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"])
+    o.init_om2(O.k4_spectrum(N, WORKLOAD["K0"], WORKLOAD["seed"]))
+    O.write_restart_v2(path, o, WORKLOAD["Re"], WORKLOAD["K0"], WORKLOAD["CFL"])
+    o.close()
+    return f"seeded k^4 exp(-2(k/K0)^2) field (seed {WORKLOAD['seed']}) via restart.bin v2 written by the FP64 oracle " \
+           f"({time.perf_counter() - t0:.1f} s, outside the timed runs)"
+
+
+def main_reference(args, runs: int = 3):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import tempfile
     N, K, W = args.n, args.steps, args.warmup
+    up = WORKLOAD["UPDATE"]
     exe = os.path.join(REPO, "oracle", "_ref", "mem_cuda")
     base = {"impl": "reference", "metric": METRIC, "unit": "steps/s", "n_gpus": 1, "steps": K,
             "warmup": W, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": workload_text(N), "N": N}}
-    if os.path.exists(exe):
-        env = dict(os.environ, BENCH_WARMUP_STEPS=str(W))
-        cmd = [exe, str(N), f"{WORKLOAD['Re']:.0E}", f"{WORKLOAD['K0']:g}", str(W + K), f"{WORKLOAD['CFL']:g}",
-               str(WORKLOAD["UPDATE"]), "0"]
-        t0 = time.perf_counter()
-        p = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
-        wall = time.perf_counter() - t0
-        m = re.search(r"Steady FPS:\s*([0-9.eE+-]+)", p.stdout)
-        if p.returncode != 0 or not m:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              f"reference mem_cuda failed rc={p.returncode}: {p.stderr[-200:]}"}))
-            return
-        v = float(m.group(1))
-        line = dict(base, value=v, ms_per_step=1e3 / v, vs_baseline=None,
-                    mpts_steps_per_s=round(v * N * N / 1e6, 1),
-                    cpu_baseline={"value": v, "unit": "steps/s", "cores": 1, "kind": "reference",
-                                  "sample": f"reference cuFFT build (oracle/_ref/mem_cuda, sm_100a) "
-                                            f"{' '.join(cmd[1:])}, BENCH_WARMUP_STEPS={W}; its own "
-                                            f"'Steady FPS' over {K} steps on cuda:0 ({wall:.1f} s wall)",
-                                  "device": "cuda:0"},
-                    e2e={"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
-        line["config"]["reference_ic"] = "PAO-k^-3 (the reference CLI's own initialiser)"
+    if not os.path.exists(exe):
+        cb = cpu_baseline(args)
+        line = dict(base, value=cb["value"], ms_per_step=1e3 / cb["value"], vs_baseline=None, cpu_baseline=cb,
+                    e2e={"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        line["config"]["reference_note"] = "reference binary not built (oracle/_ref/mem_cuda); FP64 oracle timed instead"
         print(json.dumps(line), flush=True)
         return
-    cb = cpu_baseline(args)
-    line = dict(base, value=cb["value"], ms_per_step=1e3 / cb["value"], vs_baseline=None,
-                cpu_baseline=cb,
-                e2e={"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    warm, steps_total = reference_cadence(W, K, up)
+    with tempfile.TemporaryDirectory(prefix="dns2d_refarm_") as tmp:
+        argv = [N, f"{WORKLOAD['Re']:.0E}", f"{WORKLOAD['K0']:g}", steps_total, f"{WORKLOAD['CFL']:g}", up, 0]
+        try:
+            if args.workload == "dns4096":
+                ic = reference_initial_field(N, os.path.join(tmp, "restart.bin"))
+                argv.append(os.path.join(tmp, "restart.bin"))
+            else:
+                ic = "PAO-k^-3 (the reference CLI's own initialiser; the FP64 oracle cannot hold this size)"
+            res = [run_reference_binary(exe, argv, warm, tmp) for _ in range(runs)]
+        except (RuntimeError, OSError, subprocess.TimeoutExpired, MemoryError) as e:
+            print(json.dumps({"impl": "reference", "unavailable": str(e)[:600]}), flush=True)
+            return
+    vals = sorted(r[0] for r in res)
+    v = statistics.median(vals)
+    steady = res[0][1]
+    line = dict(base, value=round(v, 3), ms_per_step=round(1e3 / v, 5), vs_baseline=None,
+                mpts_steps_per_s=round(v * N * N / 1e6, 1),
+                runs=[round(x, 3) for x in vals],
+                cpu_baseline={"value": round(v, 3), "unit": "steps/s", "cores": 1, "kind": "reference",
+                              "sample": f"reference cuFFT build (oracle/_ref/mem_cuda, sm_100a, unmodified source) "
+                                        f"{' '.join(map(str, argv[:7]))} [restart.bin], BENCH_WARMUP_STEPS={warm}; "
+                                        f"median of {runs} runs of its own 'Steady FPS' over {steady} steps on cuda:0 "
+                                        f"(one host thread driving the GPU; {sum(r[2] for r in res):.1f} s wall)",
+                              "device": "cuda:0"},
+                e2e={"value": round(v, 3), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    line["config"]["reference_ic"] = ic
+    line["config"]["steady_window"] = f"steps {warm + 1}..{steps_total} ({steady} steps), diagnostics every {up} " \
+                                      f"steps and at the last step, as in our arm's window"
     print(json.dumps(line), flush=True)
 
 
@@ -483,9 +578,35 @@ def main_ensemble(args):
     b.close()
 
 
+def main_profile(args):
+    """The short runs the ncu summaries under profiles/ were captured from."""
+    import numpy as np
+    import optimizec_b200 as P
+    if args.profile == "closure":
+        s = P.Solver(256, 1e5, 4.0, 0.1)
+        s.init_k4(1)
+        s.next_dt()
+        net = P.CNN(6, 32, seed=1)
+        s.attach_closure(net, np.array([5.0, 1.0, 1.0, 0.01], np.float32), energy_check=1)
+        s.step(3)
+        s.sync()
+        print("profile run done", s.closure_stats())
+        return
+    s = P.Solver(args.n, 1e5, 4.0, 0.1)
+    s.init_k4(1)
+    s.next_dt()
+    s.step(1)
+    s.next_dt()
+    s.step(3)
+    s.sync()
+    print("profile run done, it =", s.scalars()["it"])
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.workload == "ensemble" and a.impl == "ours":
+    if a.profile:
+        main_profile(a)
+    elif a.workload == "ensemble" and a.impl == "ours":
         main_ensemble(a)
     elif a.workload == "ensemble":
         if int(os.environ.get("RANK", "0")) == 0:

@@ -143,11 +143,13 @@ int dns2d_movie_frame(dns2d_state *s, int comp, int scale_f, unsigned char *rgb,
  *              (the reference's CNM1 <- CN rule); stream is a cudaStream_t (NULL = default)
  * Nothing is allocated: all scratch (about 20 N^2 bytes) lives in one static device array of
  * DNS2D_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until the process exits,
- * which limits N to DNS2D_NOALLOC_MAX_N; larger N returns DNS2D_ERR_SIZE.  The first call on a
- * device looks up that array's device address (with the device current), so make the first call
- * before any stream capture.  Every call shares the array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.  The call is asynchronous
- * on the stream; the host scalars (t, it, cnm1) are the caller's to advance. */
+ * which limits N to DNS2D_NOALLOC_MAX_N; larger N returns DNS2D_ERR_SIZE.  A call looks up that
+ * array's device address with the device current; while the stream is capturing it reuses the
+ * address found by the last call outside capture, so make the first call on a device before any
+ * stream capture.  Every call shares the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.  An error already pending on the
+ * calling thread is cleared on entry and not reported.  The call is asynchronous on the stream;
+ * the host scalars (t, it, cnm1) are the caller's to advance. */
 #define DNS2D_NOALLOC_MAX_N 512
 #define DNS2D_NOALLOC_SCRATCH_BYTES (6u << 20)
 int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float cn, int nsteps,

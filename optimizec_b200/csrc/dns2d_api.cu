@@ -3221,8 +3221,13 @@ namespace {
 // one array per device, allocated when the module loads and held until the process exits
 static __device__ __align__(256) unsigned char g_noalloc_scratch[DNS2D_NOALLOC_SCRATCH_BYTES];
 
-// per-device address of g_noalloc_scratch, looked up once per device with that device current
-unsigned char *noalloc_scratch_address(int *err)
+// Per-device address of g_noalloc_scratch.  In host code the array's name is only a host-side
+// stand-in, so the device address is looked up with cudaGetSymbolAddress, with the device
+// current.  Outside stream capture the lookup is repeated on every call (it is a host-side
+// query), so a context that was reset and reloaded the module at another address is never
+// handed a stale pointer; while `stream` is capturing, the address cached by the last call
+// outside capture is used.
+unsigned char *noalloc_scratch_address(cudaStream_t stream, int *err)
 {
     static std::mutex mu;
     static unsigned char *addr[128] = {};
@@ -3232,8 +3237,13 @@ unsigned char *noalloc_scratch_address(int *err)
         *err = DNS2D_ERR_CUDA;
         return nullptr;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+        *err = DNS2D_ERR_CUDA;
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone || !addr[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -3286,11 +3296,14 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     const size_t o_hist = o_cnt + align256(sizeof(unsigned int));
     const size_t total = o_hist + align256(sizeof(double2));
     if (total > DNS2D_NOALLOC_SCRATCH_BYTES) return DNS2D_ERR_SIZE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // an error left pending on this thread by earlier, unrelated launches is cleared here, so
+    // the checks below report only this call's own launches
+    (void)cudaGetLastError();
     int err = DNS2D_OK;
-    unsigned char *base = noalloc_scratch_address(&err);
+    unsigned char *base = noalloc_scratch_address(st, &err);
     if (!base) return err;
     if (ks->setup() != cudaSuccess) return DNS2D_ERR_CUDA;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     Pointers p;
     p.work = reinterpret_cast<float2 *>(base + o_work);
     p.om2 = reinterpret_cast<float2 *>(base + o_om);
@@ -3315,9 +3328,11 @@ extern "C" int dns2d_step_noalloc(int N, float visc, float dt, float cnm1, float
     k_transpose_c64<<<dim3((unsigned)((H + 31) / 32), (unsigned)((N + 31) / 32)), tb, 0, st>>>(
         static_cast<const float2 *>(fnm1), p.fnm1, N, (int)H);
     ks->cols_init(p, nullptr, 1, st, 1);  // velocity of the given vorticity
+    if (cudaGetLastError() != cudaSuccess) return DNS2D_ERR_CUDA;  // set-up launches
     for (int i = 0; i < nsteps; ++i) {
         ks->rows_step(p, st, 1);
         ks->cols_step(p, i == 0 ? 1 : 0, 0, st, 1);
+        if (cudaGetLastError() != cudaSuccess) return DNS2D_ERR_CUDA;  // step launches
     }
     k_transpose_c64<<<dim3((unsigned)((N + 31) / 32), (unsigned)((H + 31) / 32)), tb, 0, st>>>(
         p.om2, static_cast<float2 *>(om2), (int)H, N);

@@ -197,6 +197,32 @@ def threads() -> int:
     return lib().orc_threads()
 
 
+def write_restart_v2(path: str, o: "Oracle", Re: float, K0: float, cflnum: float) -> int:
+    """Write the oracle's current state as a restart.bin v2 file that the reference's own
+    mem_cuda loads unchanged (header: cuda/mem_cuda.cu:1019-1054; payload order UR_full f32
+    [3][L][L], OM2 c64 [N][N/2], FNM1 c64 [N][N/2]: cuda/mem_cuda.cu:1236-1285).  This is how one
+    seeded field reaches the reference without a change to its source.  UR plane 2 is written as
+    zeros: the reference's next step overwrites it with the uw product before reading it.
+    Returns the number of bytes written."""
+    import struct
+    N, L = o.N, o.L
+    sc = o.scalars()
+    Nk = 3 * N // 4 + 1
+    hdr = struct.pack("<16s4I10i9f4x4Q", b"CTRB_RESTART", 2, 144, 4, 8,
+                      N, N, N, N, Nk, L, L, Nk, int(sc["it"]), 1,
+                      Re, K0, sc["visc"], sc["t"], sc["dt"], sc["cn"], sc["cnm1"], cflnum, sc["cflm"],
+                      0, N * (N // 2), N * (N // 2), 3 * L * L)
+    assert len(hdr) == 144
+    with open(path, "wb") as f:
+        f.write(hdr)
+        for c in (0, 1):
+            f.write(o.ur(c).astype(np.float32).tobytes())
+        f.write(np.zeros((L, L), dtype=np.float32).tobytes())
+        f.write(o.om2().astype(np.complex64).tobytes())
+        f.write(o.fnm1().astype(np.complex64).tobytes())
+    return 144 + 3 * L * L * 4 + 2 * N * (N // 2) * 8
+
+
 class Oracle:
     """FP64 solver state mirroring the reference's DnsDeviceState + mem_cuda loop."""
 

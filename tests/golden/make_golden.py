@@ -55,7 +55,8 @@ def parse(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout: first argument, else $REF, else the build container's copy
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF", "/root/reference")
     out = {"source": "cudaturbo reference stdout (RTX 3090 runs)", "runs": []}
     for name in RUNS:
         out["runs"].append(parse(os.path.join(ref, name)))

@@ -53,3 +53,71 @@ def test_ensemble_reference_arm_is_unavailable():
     assert out.returncode == 0, out.stderr
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+@pytest.mark.parametrize("W,K,up,warm,total", [(5, 20, 100, 1, 21), (100, 500, 100, 100, 600), (250, 20, 100, 200, 220),
+                                              (20, 21, 20, 20, 41), (3, 2, 100, 1, 3)])
+def test_reference_cadence(W, K, up, warm, total):
+    import bench
+    assert bench.reference_cadence(W, K, up) == (warm, total)
+
+
+# Stands in for the reference's mem_cuda: the same steady-timer rule (cuda/mem_cuda.cu:1859,
+# 1912-1920: the timer starts inside a diagnostic step it == 1, it % UPDATE == 0 or it == STEPS,
+# once it >= BENCH_WARMUP_STEPS) and the same end-of-run lines (:2024-2036).
+FAKE_MEM_CUDA = r'''#!/usr/bin/env python3
+import os, sys
+steps, update = int(sys.argv[4]), int(sys.argv[6])
+warm = int(os.environ.get("BENCH_WARMUP_STEPS", str(update)))
+start = 0 if warm <= 0 else None
+for it in range(1, steps + 1):
+    if it == 1 or it % update == 0 or it == steps:
+        print(" ITERATION %6d T=0" % it)
+        if start is None and it >= warm:
+            start = it
+print(" Frames per second (FPS)            = %12.7f" % 500.0)
+if start is not None and steps - start > 0:
+    print(" Steady frames per second (FPS)     = %12.7f  (%d steps after warmup)" % (530.25, steps - start))
+    print(" Steady FPS: %12.7f" % 530.25)
+print("[OUTPUT] Normal completion; no output files written.")
+'''
+
+
+def _fake(tmp_path):
+    exe = tmp_path / "mem_cuda"
+    exe.write_text(FAKE_MEM_CUDA)
+    exe.chmod(0o755)
+    return str(exe)
+
+
+def test_reference_arm_window_with_short_warmup(tmp_path):
+    """--steps 20 --warmup 5 at UPDATE=100: the reference's steady window covers exactly 20 steps."""
+    import bench
+    warm, total = bench.reference_cadence(5, 20, 100)
+    v, steady, _ = bench.run_reference_binary(_fake(tmp_path), [4096, "1E+05", 4, total, 0.1, 100, 0], warm,
+                                              str(tmp_path))
+    assert steady == 20 and v == pytest.approx(530.25)
+
+
+def test_reference_arm_reports_why_it_has_no_window(tmp_path):
+    """Passing the warm-up straight through (the old rule) leaves no steady window; the error
+    says which line is missing instead of 'failed rc=0'."""
+    import bench
+    with pytest.raises(RuntimeError, match="no 'Steady frames per second' line"):
+        bench.run_reference_binary(_fake(tmp_path), [4096, "1E+05", 4, 25, 0.1, 100, 0], 5, str(tmp_path))
+
+
+def test_parse_reference_stdout():
+    import bench
+    out = (" Frames per second (FPS)            =  512.1234567\n"
+           " Steady frames per second (FPS)     =  530.7654321  (500 steps after warmup)\n"
+           " Steady FPS:  530.7654321\n")
+    assert bench.parse_reference_stdout(out) == (pytest.approx(530.7654321), 500)
+    assert bench.parse_reference_stdout(" FPS: 1.0\n") is None
+
+
+def test_window_plan():
+    import bench
+    assert bench.window_plan(5, 20, 100, 0.6) == [5 + 20 * i for i in range(84)]
+    assert bench.window_plan(100, 500, 100, 0.6) == [100, 600, 1100, 1600]
+    assert len(bench.window_plan(5, 20, 100, 1e-9)) == 200

@@ -112,3 +112,33 @@ def test_staged_roundtrip_continues_exactly(tmp_path):
     s2.step(4)
     a, b = s2.om2().astype(np.complex128), s.om2().astype(np.complex128)
     assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5   # 1.7e-6 measured at N=4096
+
+
+def test_library_reads_oracle_written_restart(tmp_path):
+    """The restart.bin v2 file that the bench writes (from the FP64 oracle) for the reference's
+    loader is also read by this library: same field, same scalars, and the run continues along the
+    same trajectory as a run started from the field itself."""
+    from oracle import oracle as O
+    N, Re, K0, cfl = 256, 1e4, 4.0, 0.1
+    om = O.k4_spectrum(N, K0, 9)
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_om2(om)
+    path = str(tmp_path / "restart.bin")
+    O.write_restart_v2(path, o, Re, K0, cfl)
+    a = P().Solver(N, Re, K0, cfl)
+    a.load_restart(path)
+    assert np.array_equal(a.om2(), om)
+    sa = a.scalars()
+    assert sa["it"] == 0 and sa["dt"] == np.float32(o.scalars()["dt"])
+    b = P().Solver(N, Re, K0, cfl)
+    b.init_vorticity(om)
+    b.next_dt()
+    assert sa["dt"] == pytest.approx(b.scalars()["dt"], rel=2e-6)
+    b.set_scalars(dt=sa["dt"], visc=sa["visc"])
+    for s in (a, b):
+        s.step(1)
+        s.next_dt()
+        s.step(9)
+    x, y = a.om2().astype(np.complex128), b.om2().astype(np.complex128)
+    assert np.linalg.norm(x - y) / np.linalg.norm(y) <= 1e-6
+    o.close()

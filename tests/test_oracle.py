@@ -121,3 +121,33 @@ def test_movie_restatement_rules():
     assert [O.movie_scale(n) for n in (256, 2560, 4096, 9216, 16384, 29400)] == [1, 1, 2, 8, 12, 14]
     rgb, sigma = O.render_frame(np.full((12, 12), 3.0, np.float32), 5)
     assert rgb.shape == (3, 3, 3) and sigma == 0.0 and np.all(rgb == lut[128])
+
+
+def test_restart_v2_writer_layout(tmp_path):
+    """The oracle's restart.bin v2 writer (how the seeded field reaches the reference's own
+    loader): 144-byte header with the dims and scalars of the state, UR planes u, w of the
+    oracle's recovered velocity, OM2 equal to the seeded field, FNM1 zero."""
+    import struct
+    N, Re, K0, cfl = 16, 1e4, 4.0, 0.1
+    o = O.Oracle(N, Re, K0, cfl)
+    om = O.k4_spectrum(N, K0, 3)
+    o.init_om2(om)
+    path = tmp_path / "restart.bin"
+    n = O.write_restart_v2(str(path), o, Re, K0, cfl)
+    b = path.read_bytes()
+    L, H = 3 * N // 2, N // 2
+    assert len(b) == n == 144 + 3 * L * L * 4 + 2 * N * H * 8
+    h = struct.unpack("<16s4I10i9f4x4Q", b[:144])
+    assert h[0].rstrip(b"\0") == b"CTRB_RESTART" and h[1:5] == (2, 144, 4, 8)
+    assert h[5:15] == (N, N, N, N, 3 * N // 4 + 1, L, L, 3 * N // 4 + 1, 0, 1)
+    sc = o.scalars()
+    Re_, K0_, visc, t, dt, cn, cnm1, cflnum, cflm = h[15:24]
+    assert (t, cn, cnm1) == (0.0, 1.0, 0.0) and dt == np.float32(sc["dt"]) and dt > 0
+    assert cflm == np.float32(sc["cflm"]) and cflnum == np.float32(cfl) and Re_ == np.float32(Re)
+    assert h[24:] == (0, N * H, N * H, 3 * L * L)
+    ur = np.frombuffer(b, dtype=np.float32, count=3 * L * L, offset=144).reshape(3, L, L)
+    assert np.array_equal(ur[0], o.ur(0).astype(np.float32)) and not ur[2].any()
+    om2 = np.frombuffer(b, dtype=np.complex64, count=N * H, offset=144 + 12 * L * L).reshape(N, H)
+    assert np.array_equal(om2, om)
+    assert not np.frombuffer(b, dtype=np.complex64, offset=144 + 12 * L * L + 8 * N * H).any()
+    o.close()

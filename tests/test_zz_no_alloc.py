@@ -54,6 +54,20 @@ def test_noalloc_matches_regular_step(N):
         want_fn = s.fnm1().astype(np.complex128)
         assert rel_l2(got_fn, want_fn) <= 1e-5, call
     s.close()
+    if N <= 64:
+        # and directly against the FP64 oracle over the same 2 x n steps at the same dt
+        from oracle import oracle as O
+        sc0 = P.Solver(N, Re, K0, cfl)
+        sc0.init_vorticity(om0)
+        sc0.next_dt()
+        d = sc0.scalars()
+        sc0.close()
+        o = O.Oracle(N, Re, K0, cfl)
+        o.init_om2(om0)
+        o.set_scalars({"visc": d["visc"]})
+        o.run_fixed([d["dt"]] * (2 * n), [d["cn"]] * (2 * n))
+        assert rel_l2(got, o.om2()) <= 1e-5
+        o.close()
 
 
 def test_noalloc_rejects_sizes_beyond_its_array():
