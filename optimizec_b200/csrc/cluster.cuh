@@ -333,14 +333,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
             if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
-        const double arg = hvdt * K2;
-        const double inv = 1.0 / (1.0 + arg);
-        const float c1 = (float)((1.0 - arg) * inv);
-        const float c2 = (float)(c2n * inv);
-        const float c3 = (float)(c3n * inv);
-        const float2 om = om2c[iz];
-        const float2 fo = fnc[iz];
-        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        const float2 on = cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
         om2c[iz] = on;
         fnc[iz] = fn;
         float2 u, w;

@@ -284,6 +284,28 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p0)
 }
 
 // ------------------------------------------------------------------------------------------
+// Crank-Nicolson / Adams-Bashforth update of one mode (cuda/step3_cuda.cu:82-100):
+//   om' = ((1 - a) om + c2n FN + c3n FNM1) / (1 + a),  a = hvdt K^2,
+// with the factors formed in FP64 and each rounded once to float.  The viscous part is carried
+// as the decrement d1 = (1 - a)/(1 + a) - 1 = -2a/(1 + a), and om' = om + (d1 om + c2 FN + c3 FNM1)
+// is rounded once: rounding the multiplier (1 - a)/(1 + a) itself to float would quantise the
+// decay of the energy-bearing low-k modes, where 2a (~1e-7 K^2 at Re = 1e4) is comparable to the
+// float spacing just below 1, into a systematic energy drift of ~1e-8 per step.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 cn_update(float2 om, float2 fn, float2 fo, double K2, double hvdt, double c2n,
+                                            double c3n)
+{
+    const double arg = hvdt * K2;
+    const double inv = 1.0 / (1.0 + arg);
+    const float d1 = (float)(-2.0 * arg * inv);
+    const float c2 = (float)(c2n * inv);
+    const float c3 = (float)(c3n * inv);
+    const float ix = fmaf(d1, om.x, fmaf(c2, fn.x, c3 * fo.x));
+    const float iy = fmaf(d1, om.y, fmaf(c2, fn.y, c3 * fo.y));
+    return make_float2(om.x + ix, om.y + iy);
+}
+
+// ------------------------------------------------------------------------------------------
 // Velocity recovery of one mode (cuda/step3_cuda.cu:103-138): u = -i kz om / K^2,
 // w = i kx om / K^2; on kx = 0: u = -i om / kz (0 at kz = 0), w = 0.  The factors kz/K^2 and
 // kx/K^2 are formed in FP64 and rounded once.
@@ -353,14 +375,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
             if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
-        const double arg = hvdt * K2;
-        const double inv = 1.0 / (1.0 + arg);
-        const float c1 = (float)((1.0 - arg) * inv);
-        const float c2 = (float)(c2n * inv);
-        const float c3 = (float)(c3n * inv);
-        const float2 om = om2c[iz];
-        const float2 fo = fnc[iz];
-        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        const float2 on = cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
         om2c[iz] = on;
         fnc[iz] = fn;
         float2 u, w;
@@ -630,14 +645,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
             if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
-        const double arg = hvdt * K2;
-        const double inv = 1.0 / (1.0 + arg);
-        const float c1 = (float)((1.0 - arg) * inv);
-        const float c2 = (float)(c2n * inv);
-        const float c3 = (float)(c3n * inv);
-        const float2 om = om2c[iz];
-        const float2 fo = fnc[iz];
-        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        const float2 on = cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
         om2c[iz] = on;
         fnc[iz] = fn;
         float2 u, w;
@@ -821,14 +829,7 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
             if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
-        const double arg = hvdt * K2;
-        const double inv = 1.0 / (1.0 + arg);
-        const float c1 = (float)((1.0 - arg) * inv);
-        const float c2 = (float)(c2n * inv);
-        const float c3 = (float)(c3n * inv);
-        const float2 om = om2c[iz];
-        const float2 fo = fnc[iz];
-        const float2 on = make_float2(c1 * om.x + c2 * fn.x + c3 * fo.x, c1 * om.y + c2 * fn.y + c3 * fo.y);
+        const float2 on = cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
         om2c[iz] = on;
         fnc[iz] = fn;
         float2 u, w;

@@ -243,6 +243,7 @@ typedef struct {
     int N, H, L, Nk;
     float Re, K0, visc, t, dt, cn, cnm1, cflnum, cflm;
     int it, ifn;
+    int f32_cn; /* 1: Crank-Nicolson factors rounded in float as the reference's STEP3 forms them */
     double *ur;  /* [3][L][L] */
     zc *uc;      /* [3][L][Nk] */
     zc *om2;     /* [N][H] compact, ix fastest */
@@ -316,10 +317,20 @@ static void step3(orc_state *S)
             const int zspec = (iz < N / 2) ? iz : iz + N / 2;
             const zc u1 = UC(S, 0, zspec, ix), u2 = UC(S, 1, zspec, ix), u3 = UC(S, 2, zspec, ix);
             const zc FN = (gz * ax * (u1 - u2) + (gz * gz - ax * ax) * u3) * divxz;
-            const double ARG = 0.5 * visc * dt * K2;
-            const double DEN = 1.0 + ARG;
-            const zc om = ((1.0 - ARG) * S->om2[io] + 0.5 * dt * (2.0 + cnm1) * FN
-                           - 0.5 * dt * cnm1 * S->fnm1[io]) / DEN;
+            zc om;
+            if (S->f32_cn) {
+                /* the reference's float factors (cuda/step3_cuda.cu:82-91): VT, ARG, DEN, c1, c2, c3
+                 * each rounded to float in its operation order; the update itself in double */
+                const float VT = 0.5f * S->visc * S->dt;
+                const float ARG = VT * ((float)ix * (float)ix + (float)gz * (float)gz);
+                const float DEN = 1.0f + ARG, c1 = 1.0f - ARG;
+                const float c2 = 0.5f * S->dt * (2.0f + S->cnm1), c3 = -0.5f * S->dt * S->cnm1;
+                om = ((double)c1 * S->om2[io] + (double)c2 * FN + (double)c3 * S->fnm1[io]) / (double)DEN;
+            } else {
+                const double ARG = 0.5 * visc * dt * K2;
+                const double DEN = 1.0 + ARG;
+                om = ((1.0 - ARG) * S->om2[io] + 0.5 * dt * (2.0 + cnm1) * FN - 0.5 * dt * cnm1 * S->fnm1[io]) / DEN;
+            }
             S->om2[io] = om;
             S->fnm1[io] = FN;
             zc o1 = 0, o2 = 0;
@@ -847,6 +858,10 @@ int orc_run_fixed(orc_state *S, int nsteps, const float *dts, const float *cns, 
 /* ------------------------------------------------------------------------------------------ */
 /* Accessors                                                                                   */
 /* ------------------------------------------------------------------------------------------ */
+/* 1: form the Crank-Nicolson factors in float as the reference does (for attributing the
+ * reference's own distance from the FP64 scheme); 0 (default): FP64 */
+void orc_set_f32_cn(orc_state *S, int on) { S->f32_cn = on; }
+
 void orc_get_scalars(const orc_state *S, double *out)
 {
     out[0] = S->it; out[1] = S->t; out[2] = S->dt; out[3] = S->cn; out[4] = S->cnm1;

@@ -43,6 +43,7 @@ def lib():
         L.orc_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, dp]
         L.orc_run_fixed.argtypes = [C.c_void_p, C.c_int, fp, fp, dp, dp]
         L.orc_get_scalars.argtypes = [C.c_void_p, dp]
+        L.orc_set_f32_cn.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_scalars.argtypes = [C.c_void_p, dp]
         L.orc_get_om2.argtypes = [C.c_void_p, dp]
         L.orc_get_fnm1.argtypes = [C.c_void_p, dp]
@@ -267,6 +268,12 @@ class Oracle:
         Z = np.zeros(n)
         lib().orc_run_fixed(self._s, n, _fp(dts), _fp(cns), _dp(E), _dp(Z))
         return E, Z
+
+    def f32_cn(self, on: bool = True):
+        """Form the Crank-Nicolson factors in float, rounded in the reference's operation order
+        (cuda/step3_cuda.cu:82-91), instead of FP64: the variant that isolates how far the
+        reference's own FP32 factors move it from the FP64 scheme."""
+        lib().orc_set_f32_cn(self._s, int(on))
 
     def scalars(self) -> dict:
         v = np.zeros(8)
