@@ -269,6 +269,10 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.barrier()
     value = replica_throughput(K, ms_max, world)
 
+    E_end, Z_end = s.energy_enstrophy()
+    if not (np.isfinite(E_end) and np.isfinite(Z_end) and 0.0 < E_end < 1.0):
+        raise RuntimeError(f"the field is not a valid state after the timed steps: E={E_end} Z={Z_end}")
+
     # per-kernel device time (CUDA events around each launch, on the solver's stream)
     s.phase_timing(True)
     s.step(20)

@@ -105,7 +105,10 @@ int dns2d_energy_enstrophy(dns2d_state *s, double *E, double *Z);
 int dns2d_shell_spectrum(dns2d_state *s, double *Ek, int nbins);
 /* palinstrophy ratio of cuda/mem_cuda.cu:872-940 (FP64 on the device) */
 int dns2d_palin(dns2d_state *s, double *pal_over_ens_kmax2);
-/* energy_spectrum.csv bins of cuda/mem_cuda.cu:575-649 from phys[0..1] (nbins = 3N) */
+/* energy_spectrum.csv bins of cuda/mem_cuda.cu:575-649 (nbins = 3N): the forward R2C of the
+ * physical velocity over every mode, binned on the host in the reference's loop order, so the
+ * bins beyond the retained radius hold the transform's rounding noise as in the reference; at the
+ * cluster sizes (N >= 8192, rows beyond one CTA) only the retained modes, exactly */
 int dns2d_velocity_spectrum_bins(dns2d_state *s, double *esum, int *count, int nbins);
 
 /* ---- state transfer ---- */

@@ -550,8 +550,55 @@ const char *kStatFmt[19] = {" Reynolds n. =%12.1f\n", " Energy      =%12.7f\n", 
 
 }  // namespace
 
+// DUMP <restart.bin> <folder> [UPDATE]: write the files of a signal save (the PGMs,
+// energy_spectrum.csv, metrics.csv, meta.csv of cuda/mem_cuda.cu:1396-1449) for the state held in
+// a restart file, without stepping.  An addition of this CLI: the reference writes them only from
+// a running simulation; this renders any saved state, e.g. the restart.bin of a SIGRTMIN save.
+int dump_restart(const char *path, const char *folder, int update)
+{
+    unsigned char hdr[144];
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp || std::fread(hdr, 1, sizeof(hdr), fp) < 136) {
+        if (fp) std::fclose(fp);
+        std::fprintf(stderr, "DUMP: cannot read the header of %s\n", path);
+        return 1;
+    }
+    std::fclose(fp);
+    int32_t N = 0;
+    float Re = 0.0f, K0 = 0.0f, cfl = 0.0f;
+    std::memcpy(&N, hdr + 32, 4);  // Nbase (restart header, cuda/mem_cuda.cu:1019-1054)
+    std::memcpy(&Re, hdr + 72, 4);
+    std::memcpy(&K0, hdr + 76, 4);
+    std::memcpy(&cfl, hdr + 100, 4);
+    dns2d_state *s = nullptr;
+    int rc = dns2d_create(&s, N, Re, K0, cfl, 0);
+    if (rc) {
+        std::fprintf(stderr, "DUMP: dns2d_create(N=%d): %s\n", N, dns2d_strerror(rc));
+        return 1;
+    }
+    rc = dns2d_load_restart(s, path);
+    if (rc) {
+        std::fprintf(stderr, "DUMP: %s: %s\n", dns2d_strerror(rc), dns2d_last_error(s));
+        dns2d_destroy(s);
+        return 1;
+    }
+    dns2d_scalars sc;
+    dns2d_get_scalars(s, &sc);
+    std::printf(" DUMP of %s: N=%d it=%d T=%12.10f\n", path, N, sc.it, (double)sc.t);
+    const bool ok = dump_outputs(s, {}, folder, update, 0.0, 0.0);
+    dns2d_destroy(s);
+    return ok ? 0 : 1;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc > 1 && std::strcmp(argv[1], "DUMP") == 0) {
+        if (argc < 4) {
+            std::fprintf(stderr, "Usage: %s DUMP restart.bin output_folder [UPDATE]\n", argv[0]);
+            return 2;
+        }
+        return dump_restart(argv[2], argv[3], argc > 4 ? std::atoi(argv[4]) : 0);
+    }
     install_signals();
     int N = 512, STEPS = 1001, UPDATE = 100;
     float Re = 10000.0f, K0 = 10.0f, CFL = 0.25f;

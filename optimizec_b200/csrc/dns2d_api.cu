@@ -1393,6 +1393,46 @@ extern "C" int dns2d_shell_spectrum(dns2d_state *s, double *Ek, int nb)
 extern "C" int dns2d_velocity_spectrum_bins(dns2d_state *s, double *esum, int *count, int nbins)
 {
     if (!s || !esum || !count || nbins <= 0) return DNS2D_ERR_ARG;
+    if (s->ks->velocity_r2c_full) {
+        // the reference's procedure (cuda/mem_cuda.cu:579-649): forward R2C of the physical u, w
+        // over every mode of the L x L grid, then the shell sums on the host in its loop order
+        // (z outer, kx inner), so every bin it writes -- the retained band and the transform's
+        // rounding noise beyond it -- is formed the same way
+        const int L = s->L, NK = L / 2 + 1;
+        const size_t plane = (size_t)L * NK;
+        int rc = dns2d_velocity_phys(s);
+        if (rc) return rc;
+        float2 *d = nullptr;
+        DNS2D_CUDA(cudaMallocAsync((void **)&d, 2 * plane * sizeof(float2), s->stream), "spectrum alloc");
+        s->ks->velocity_r2c_full(s->ptrs(), s->phys, d, s->stream);
+        DNS2D_LAUNCHED("velocity r2c");
+        std::vector<float2> h(2 * plane);
+        DNS2D_CUDA(cudaMemcpyAsync(h.data(), d, 2 * plane * sizeof(float2), cudaMemcpyDeviceToHost, s->stream),
+                   "spectrum copy");
+        DNS2D_CUDA(cudaFreeAsync(d, s->stream), "spectrum free");
+        DNS2D_CUDA(cudaStreamSynchronize(s->stream), "spectrum sync");
+        std::fill(esum, esum + nbins, 0.0);
+        std::fill(count, count + nbins, 0);
+        const double r_max = std::sqrt(2.0), k_nyq = 0.5 * (double)L;
+        for (int z = 0; z < L; ++z) {
+            const int kz = (z <= L / 2) ? z : z - L;
+            for (int kx = 0; kx < NK; ++kx) {
+                if (kx == 0 && kz == 0) continue;
+                const double r = std::sqrt((double)(kx * kx + kz * kz)) / k_nyq;
+                int bin = (int)std::floor((r / r_max) * nbins);
+                bin = std::min(std::max(bin, 0), nbins - 1);
+                const float2 u = h[(size_t)z * NK + kx], v = h[plane + (size_t)z * NK + kx];
+                double p = (double)u.x * u.x + (double)u.y * u.y + (double)v.x * v.x + (double)v.y * v.y;
+                const bool dbl = kx > 0 && kx < L / 2;
+                if (dbl) p *= 2.0;
+                esum[bin] += p;
+                count[bin] += dbl ? 2 : 1;
+            }
+        }
+        return DNS2D_OK;
+    }
+    // cluster sizes: the retained modes from the spectral state (exact; the bins beyond the
+    // retained radius, which hold only transform rounding noise, stay empty)
     double *d = nullptr;
     int *c = nullptr;
     DNS2D_CUDA(cudaMallocAsync((void **)&d, (size_t)nbins * 8, s->stream), "bins alloc");

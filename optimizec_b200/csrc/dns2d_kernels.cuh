@@ -435,20 +435,25 @@ struct Cfg2 {
     static constexpr bool enabled = false;
 };
 
-#define DNS2D_CFG2(N_, NT_, R1_, R2_, R3_, MC2_, MC4_)                                         \
+#define DNS2D_CFG2(N_, NT_, R1_, R2_, R3_, MC2_, MC4_, PS_)                                    \
     template <>                                                                                \
     struct Cfg2<N_> {                                                                          \
         static constexpr bool enabled = true;                                                  \
-        static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, LP = SmemLen<L>::value;       \
+        static constexpr int PS = PS_; /* shared-memory padding: one float2 every 2^PS */       \
+        static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, LP = SmemLen<L, PS_>::value;  \
         static constexpr int NT = NT_, R1 = R1_, R2 = R2_, R3 = R3_;                           \
         static constexpr int MC2 = MC2_, MC4 = MC4_; /* CTAs per SM: k_cols_step2, k_cols_step4 */ \
         static_assert(R1_ * R2_ * R3_ == L, "plan");                                           \
         static_assert(L / R1_ <= NT_ && L / R2_ <= NT_ && L / R3_ <= NT_, "one butterfly");    \
     };
-//          N    NT  plan (R1, R2, R3)  column CTAs per SM asked of the register allocator
-DNS2D_CFG2(1024, 192, 16, 8, 12,       2, 1)
-DNS2D_CFG2(2048, 256, 16, 16, 12,      2, 2)  // two-group columns at 64 registers, 2 CTAs per SM
-DNS2D_CFG2(4096, 384, 16, 16, 24,      2, 1)
+// N = 4096: plan (16, 24, 16) with padding every 16 elements makes every shared-memory access of
+// both passes bank-conflict free (the radix-24 stage has Ns = 16, so its stores are contiguous per
+// half-warp, and the stride-16 stores of the Ns = 1 stages spread over all banks); the radix-16
+// middle stage of the row pass also holds 16 values in registers instead of 24.
+//          N    NT  plan (R1, R2, R3)  column CTAs per SM asked of the register allocator, pad
+DNS2D_CFG2(1024, 192, 16, 8, 12,       2, 1, 5)
+DNS2D_CFG2(2048, 256, 16, 16, 12,      2, 2, 5)  // two-group columns at 64 registers, 2 CTAs per SM
+DNS2D_CFG2(4096, 384, 16, 24, 16,      2, 1, 4)
 #undef DNS2D_CFG2
 
 // twiddle catalog of size N: the stages of every plan compiled for it
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
-    constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3;
+    constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS;
     constexpr int LR1 = L / R1, LR3 = L / R3;
     extern __shared__ float2 s[];
     const int z = blockIdx.x;
@@ -551,30 +556,30 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
             }
         }
         DFT<R1, true>::run(v);
-        sm_store<L, R1, 1>(s, v, jb);
+        sm_store<L, R1, 1, PS>(s, v, jb);
     }
-    stage1<TwCat<N>, L, R2, R1, true>(s, p.tw);
+    stage1<TwCat<N>, L, R2, R1, true, PS>(s, p.tw);
     // inverse stage 3 into registers -> products -> forward stage 1
     float2 v[R3];
     __syncthreads();
     if (j < LR3) {
-        sm_load<L, R3>(v, s, j);
+        sm_load<L, R3, PS>(v, s, j);
         bfly<TwCat<N>, L, R3, LR3, true>(v, j, p.tw);
 #pragma unroll
         for (int q = 0; q < R3; ++q) v[q] = make_float2(v[q].x * v[q].x - v[q].y * v[q].y, 2.0f * v[q].x * v[q].y);
         DFT<R3, false>::run(v);
     }
     __syncthreads();
-    if (j < LR3) sm_store<L, R3, 1>(s, v, j);
-    stage1<TwCat<N>, L, R2, R3, false>(s, p.tw);
+    if (j < LR3) sm_store<L, R3, 1, PS>(s, v, j);
+    stage1<TwCat<N>, L, R2, R3, false, PS>(s, p.tw);
     // the unpack reads Q[k] and Q[L-k] for k < H: positions in [H, L-H] are never read
-    stage1_last_band<TwCat<N>, L, R1, false, H, L - H>(s, p.tw);
+    stage1_last_band<TwCat<N>, L, R1, false, H, L - H, PS>(s, p.tw);
     __syncthreads();
     float2 *__restrict__ Do = p.work + widx<L, H>(0, z, 0);
     float2 *__restrict__ Eo = p.work + widx<L, H>(1, z, 0);
     for (int k = j; k < H; k += C::NT) {
-        const float2 q = s[sidx(k)];
-        const float2 m = s[sidx(k == 0 ? 0 : L - k)];
+        const float2 q = s[sidx<PS>(k)];
+        const float2 m = s[sidx<PS>(k == 0 ? 0 : L - k)];
         Do[(size_t)k << 2] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
         Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
     }
@@ -585,7 +590,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
-    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS;
     constexpr int LR1 = L / R1, LR3 = L / R3;
     extern __shared__ float2 smem[];
     __shared__ double2 red[32];
@@ -615,10 +620,10 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
 #pragma unroll
             for (int r = 0; r < R3; ++r, ptr += RS) v[r] = *ptr;
             DFT<R3, false>::run(v);
-            sm_store<L, R3, 1>(s, v, j);
+            sm_store<L, R3, 1, PS>(s, v, j);
         }
-        stage1<TwCat<N>, L, R2, R3, false>(s, p.tw);
-        stage1<TwCat<N>, L, R1, R3 * R2, false>(s, p.tw);
+        stage1<TwCat<N>, L, R2, R3, false, PS>(s, p.tw);
+        stage1<TwCat<N>, L, R1, R3 * R2, false, PS>(s, p.tw);
     }
     __syncthreads();
 
@@ -634,8 +639,8 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
     for (int iz = j; iz < N; iz += NT) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
-        const float2 d = sD[sidx(kzi)];
-        const float2 e = sE[sidx(kzi)];
+        const float2 d = sD[sidx<PS>(kzi)];
+        const float2 e = sE[sidx<PS>(kzi)];
         float2 fn = make_float2(0.f, 0.f);
         if (kz != -H) {
             const float ga = (float)kz * (float)kx;
@@ -651,15 +656,15 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
         float2 u, w;
         double invK2;
         recover_velocity(kx, kz, on, u, w, invK2);
-        sD[sidx(kzi)] = u;
-        sE[sidx(kzi)] = w;
+        sD[sidx<PS>(kzi)] = u;
+        sE[sidx<PS>(kzi)] = w;
         const double pw = (double)on.x * on.x + (double)on.y * on.y;
         ez.x += wgt * pw * invK2;
         ez.y += wgt * pw;
     }
     for (int z = H + j; z < L - H; z += NT) {
-        sD[sidx(z)] = make_float2(0.f, 0.f);
-        sE[sidx(z)] = make_float2(0.f, 0.f);
+        sD[sidx<PS>(z)] = make_float2(0.f, 0.f);
+        sE[sidx<PS>(z)] = make_float2(0.f, 0.f);
     }
     ez = block_sum2<NT>(ez, red);
     if (threadIdx.x == 0) {
@@ -686,12 +691,12 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, Cfg2<N>::MC2) k_cols_step2(Pointe
 #pragma unroll 1
     for (int a = 0; a < 2; ++a) {
         float2 *s = a ? sE : sD;
-        stage1<TwCat<N>, L, R3, 1, true>(s, p.tw);
-        stage1<TwCat<N>, L, R2, R3, true>(s, p.tw);
+        stage1<TwCat<N>, L, R3, 1, true, PS>(s, p.tw);
+        stage1<TwCat<N>, L, R2, R3, true, PS>(s, p.tw);
         __syncthreads();
         if (j < LR1) {
             float2 v[R1];
-            sm_load<L, R1>(v, s, j);
+            sm_load<L, R1, PS>(v, s, j);
             bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
             static_assert(LR1 % 4 == 0, "stride");
             constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
@@ -717,23 +722,23 @@ __device__ __forceinline__ void group_sync(int id)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NTH) : "memory");
 }
 
-template <class Cat, int L, int R, int NS, bool INV, int NTH>
+template <class Cat, int L, int R, int NS, bool INV, int NTH, int PS = 5>
 __device__ __forceinline__ void stage1g(float2 *s, const float2 *tw, int j, int bar)
 {
     constexpr int LR = L / R;
     float2 v[R];
     group_sync<NTH>(bar);
     if (j < LR) {
-        sm_load<L, R>(v, s, j);
+        sm_load<L, R, PS>(v, s, j);
         bfly<Cat, L, R, NS, INV>(v, j, tw);
     }
     group_sync<NTH>(bar);
-    if (j < LR) sm_store<L, R, NS>(s, v, j);
+    if (j < LR) sm_store<L, R, NS, PS>(s, v, j);
 }
 
 // group stage variants with a compile-time band [B0, B1]: a first stage (Ns = 1) whose inputs in
 // the band are zero, and a last stage (Ns = L/R) whose outputs in the band are never read
-template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1>
+template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1, int PS = 5>
 __device__ __forceinline__ void stage1g_first_band(float2 *s, const float2 *tw, int j, int bar)
 {
     constexpr int LR = L / R;
@@ -742,28 +747,28 @@ __device__ __forceinline__ void stage1g_first_band(float2 *s, const float2 *tw, 
     if (j < LR) {
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            v[r] = slot_in_band<L, R, B0, B1>(r) ? make_float2(0.f, 0.f) : s[sidx(j + r * LR)];
+            v[r] = slot_in_band<L, R, B0, B1>(r) ? make_float2(0.f, 0.f) : s[sidx<PS>(j + r * LR)];
         DFT<R, INV>::run(v);
     }
     group_sync<NTH>(bar);
-    if (j < LR) sm_store<L, R, 1>(s, v, j);
+    if (j < LR) sm_store<L, R, 1, PS>(s, v, j);
 }
 
-template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1>
+template <class Cat, int L, int R, bool INV, int NTH, int B0, int B1, int PS = 5>
 __device__ __forceinline__ void stage1g_last_band(float2 *s, const float2 *tw, int j, int bar)
 {
     constexpr int LR = L / R;
     float2 v[R];
     group_sync<NTH>(bar);
     if (j < LR) {
-        sm_load<L, R>(v, s, j);
+        sm_load<L, R, PS>(v, s, j);
         bfly<Cat, L, R, LR, INV>(v, j, tw);
     }
     group_sync<NTH>(bar);
     if (j < LR) {
 #pragma unroll
         for (int q = 0; q < R; ++q)
-            if (!slot_in_band<L, R, B0, B1>(q)) s[sidx(j + q * LR)] = v[q];
+            if (!slot_in_band<L, R, B0, B1>(q)) s[sidx<PS>(j + q * LR)] = v[q];
     }
 }
 
@@ -772,7 +777,7 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
-    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, NT2 = 2 * C::NT;
+    constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NT, NT2 = 2 * C::NT, PS = C::PS;
     constexpr int R1 = C::R1, R2 = C::R2, R3 = C::R3, LR1 = L / R1;
     static_assert(NT % 32 == 0, "groups must be whole warps");
     extern __shared__ float2 smem[];
@@ -786,7 +791,7 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
     float2 *sg = smem + g * LP;
     float2 *om2c = p.om2 + (size_t)kx * N;
     float2 *fnc = p.fnm1 + (size_t)kx * N;
-    for (int z = j; z < L; z += NT) cp_async8(sg + sidx(z), p.work + widx<L, H>(g, z, kx));
+    for (int z = j; z < L; z += NT) cp_async8(sg + sidx<PS>(z), p.work + widx<L, H>(g, z, kx));
     cp_async_commit();
     for (int o = (int)threadIdx.x * 16; o < N; o += NT2 * 16) {
         prefetch_l2(om2c + o);
@@ -800,10 +805,10 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
         }
     }
     cp_async_wait<0>();
-    stage1g<TwCat<N>, L, R3, 1, false, NT>(sg, p.tw, j, bar);
-    stage1g<TwCat<N>, L, R2, R3, false, NT>(sg, p.tw, j, bar);
+    stage1g<TwCat<N>, L, R3, 1, false, NT, PS>(sg, p.tw, j, bar);
+    stage1g<TwCat<N>, L, R2, R3, false, NT, PS>(sg, p.tw, j, bar);
     // the update reads kz_i < H and kz_i >= L - H only: the 3/2 band [H, L-H-1] is not stored
-    stage1g_last_band<TwCat<N>, L, R1, false, NT, H, L - H - 1>(sg, p.tw, j, bar);
+    stage1g_last_band<TwCat<N>, L, R1, false, NT, H, L - H - 1, PS>(sg, p.tw, j, bar);
     __syncthreads();
 
     const StepParams prm = *p.prm;
@@ -818,8 +823,8 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
     for (int iz = (int)threadIdx.x; iz < N; iz += NT2) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
-        const float2 d = sD[sidx(kzi)];
-        const float2 e = sE[sidx(kzi)];
+        const float2 d = sD[sidx<PS>(kzi)];
+        const float2 e = sE[sidx<PS>(kzi)];
         float2 fn = make_float2(0.f, 0.f);
         if (kz != -H) {
             const float ga = (float)kz * (float)kx;
@@ -835,8 +840,8 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
         float2 u, w;
         double invK2;
         recover_velocity(kx, kz, on, u, w, invK2);
-        sD[sidx(kzi)] = u;
-        sE[sidx(kzi)] = w;
+        sD[sidx<PS>(kzi)] = u;
+        sE[sidx<PS>(kzi)] = w;
         const double pw = (double)on.x * on.x + (double)on.y * on.y;
         ez.x += wgt * pw * invK2;
         ez.y += wgt * pw;
@@ -862,15 +867,24 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
             *p.counter = 0u;
         }
     }
+    // 3/2 zero padding: the band [H, L-H-1] enters the first inverse stage as compile-time zeros
+    // where whole radix-R3 slots lie in it; band positions in a slot that also holds retained
+    // modes are read from shared memory, so they are cleared here (none when the slots tile the
+    // band exactly, as with R3 = 12 or 24)
+    for (int z = H + (int)threadIdx.x; z < L - H; z += NT2) {
+        if (!slot_in_band<L, R3, H, L - H - 1>(z / (L / R3))) {
+            sD[sidx<PS>(z)] = make_float2(0.f, 0.f);
+            sE[sidx<PS>(z)] = make_float2(0.f, 0.f);
+        }
+    }
     __syncthreads();
     // inverse transform of this group's column, plan (R3, R2, R1), last stage straight to HBM
-    // 3/2 zero padding: the band [H, L-H-1] enters the first stage as compile-time zeros
-    stage1g_first_band<TwCat<N>, L, R3, true, NT, H, L - H - 1>(sg, p.tw, j, bar);
-    stage1g<TwCat<N>, L, R2, R3, true, NT>(sg, p.tw, j, bar);
+    stage1g_first_band<TwCat<N>, L, R3, true, NT, H, L - H - 1, PS>(sg, p.tw, j, bar);
+    stage1g<TwCat<N>, L, R2, R3, true, NT, PS>(sg, p.tw, j, bar);
     group_sync<NT>(bar);
     if (j < LR1) {
         float2 v[R1];
-        sm_load<L, R1>(v, sg, j);
+        sm_load<L, R1, PS>(v, sg, j);
         bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
         static_assert(LR1 % 4 == 0, "stride");
         constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
@@ -1105,6 +1119,51 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_fwd_scalar(Pointers p, con
         const float2 v = smem[sidx(kzi)];
         out[(size_t)kx * N + iz] = (kz == -H) ? make_float2(0.f, 0.f) : make_float2(v.x * sc, v.y * sc);
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// Dump path: the unnormalised forward 2D R2C of the physical velocity planes u, w, every mode
+// kx in [0, L/2], kz in [0, L) -- the transform the reference's energy_spectrum.csv is binned
+// from (cuda/mem_cuda.cu:579-581).  Output spec[c][z][kx] complex64, pitch L/2 + 1.
+// Rows: u + i w through one complex FFT per row, U = (Q[k] + conj Q[L-k]) / 2,
+// W = (Q[k] - conj Q[L-k]) / 2i; columns: one forward C2C per (kx, component).
+// ------------------------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_r2c_full(Pointers p, const float *phys, float2 *spec)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, LP = C::LP, ROWS = C::ROWS, NT = C::NTB, NK = L / 2 + 1;
+    extern __shared__ float2 smem[];
+    const int z0 = blockIdx.x * ROWS;
+    const float *u = phys, *w = phys + (size_t)L * L;
+    for (int e = threadIdx.x; e < ROWS * L; e += NT) {
+        const int r = e / L, x = e - r * L;
+        const size_t i = (size_t)(z0 + r) * L + x;
+        smem[r * LP + sidx(x)] = make_float2(u[i], w[i]);
+    }
+    __syncthreads();
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    for (int e = threadIdx.x; e < ROWS * NK; e += NT) {
+        const int r = e / NK, k = e - r * NK;
+        const float2 q = smem[r * LP + sidx(k)];
+        const float2 m = smem[r * LP + sidx(k == 0 ? 0 : L - k)];
+        const size_t o = (size_t)(z0 + r) * NK + k;
+        spec[o] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
+        spec[(size_t)L * NK + o] = make_float2(0.5f * (q.y + m.y), -0.5f * (q.x - m.x));
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_c2c_full(Pointers p, float2 *spec)
+{
+    using C = Cfg<N>;
+    constexpr int L = C::L, LP = C::LP, NT = C::NTA, NK = L / 2 + 1;
+    extern __shared__ float2 smem[];
+    float2 *col = spec + (size_t)blockIdx.y * L * NK + blockIdx.x;
+    for (int z = threadIdx.x; z < L; z += NT) smem[sidx(z)] = col[(size_t)z * NK];
+    __syncthreads();
+    fft_run<TwCat<N>, L, LP, false, 1, NT>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) col[(size_t)z * NK] = smem[sidx(z)];
 }
 
 }  // namespace dns2d

@@ -247,15 +247,18 @@ struct DFT {
 };
 
 // ------------------------------------------------------------------------------------------
-// Shared-memory layout: one float2 of padding every 32 elements (bank-conflict-free strided
-// butterfly writes for radix 8/16), and a per-array stride that shifts consecutive arrays by
-// 8 banks.
+// Shared-memory layout: one float2 of padding every 2^PS elements (PS = 5 by default: bank-
+// conflict-free strided butterfly writes for radix 8/16; a plan whose first stage writes at
+// stride 16 uses PS = 4), and a per-array stride that shifts consecutive arrays by 8 banks.
+// A warp's 8-byte accesses are served per half-warp: conflict-free when the 16 padded indices of
+// a half-warp are distinct modulo 16.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ int sidx(int i) { return i + (i >> 5); }
+template <int PS = 5>
+__device__ __forceinline__ int sidx(int i) { return i + (i >> PS); }
 
-template <int L>
+template <int L, int PS = 5>
 struct SmemLen {
-    static constexpr int raw = L + (L >> 5) + 1;
+    static constexpr int raw = L + (L >> PS) + 1;
     static constexpr int value = ((raw + 15) / 16) * 16 + 4;
 };
 
@@ -387,48 +390,49 @@ __device__ __forceinline__ void bfly(float2 (&v)[R], int j, const float2 *__rest
 #define DNS2D_IDX 1
 #endif
 
-// Butterfly j reads x[j + r L/R].  When L/R is a multiple of 32 the padded index is
-// sidx(j) + r (L/R + L/R/32): one address, the rest compile-time offsets.
-template <int L, int R>
+// Butterfly j reads x[j + r L/R].  When L/R is a multiple of G = 2^PS the padded index is
+// sidx(j) + r (L/R + L/R/G): one address, the rest compile-time offsets.
+template <int L, int R, int PS = 5>
 __device__ __forceinline__ void sm_load(float2 (&v)[R], const float2 *__restrict__ x, int j)
 {
-    constexpr int LR = L / R;
-    if constexpr (DNS2D_IDX && LR % 32 == 0) {
-        const float2 *__restrict__ b = x + sidx(j);
+    constexpr int LR = L / R, G = 1 << PS;
+    if constexpr (DNS2D_IDX && LR % G == 0) {
+        const float2 *__restrict__ b = x + sidx<PS>(j);
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = b[r * (LR + LR / 32)];
+        for (int r = 0; r < R; ++r) v[r] = b[r * (LR + LR / G)];
     } else {
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = x[sidx(j + r * LR)];
+        for (int r = 0; r < R; ++r) v[r] = x[sidx<PS>(j + r * LR)];
     }
 }
 
 // Butterfly j writes y[A + k + q Ns], A = (j / Ns) Ns R, k = j % Ns.  Compile-time offsets from
-// one address when the 32-element padding groups allow it:
-//   Ns % 32 == 0:                   sidx(A + k) + q (Ns + Ns/32)
-//   32 % Ns == 0, (Ns R) % 32 == 0: A + A/32 + k + q Ns + (q Ns)/32   (k + q Ns never crosses a group)
-//   Ns == 1, 32 % R == 0:           sidx(A) + q                       (A .. A+R-1 in one group)
-template <int L, int R, int NS>
+// one address when the G-element padding groups (G = 2^PS) allow it:
+//   Ns % G == 0:                  sidx(A + k) + q (Ns + Ns/G)
+//   G % Ns == 0, (Ns R) % G == 0: A + A/G + k + q Ns + (q Ns)/G   (k + q Ns never crosses a group)
+//   Ns == 1, G % R == 0:          sidx(A) + q                     (A .. A+R-1 in one group)
+template <int L, int R, int NS, int PS = 5>
 __device__ __forceinline__ void sm_store(float2 *__restrict__ y, const float2 (&v)[R], int j)
 {
+    constexpr int G = 1 << PS;
     const int k = j % NS;
     const int A = (j / NS) * NS * R;
-    if constexpr (DNS2D_IDX && NS % 32 == 0) {
-        float2 *__restrict__ b = y + sidx(A + k);
+    if constexpr (DNS2D_IDX && NS % G == 0) {
+        float2 *__restrict__ b = y + sidx<PS>(A + k);
 #pragma unroll
-        for (int q = 0; q < R; ++q) b[q * (NS + NS / 32)] = v[q];
-    } else if constexpr (DNS2D_IDX && 32 % NS == 0 && (NS * R) % 32 == 0) {
-        float2 *__restrict__ b = y + A + (A >> 5) + k;
+        for (int q = 0; q < R; ++q) b[q * (NS + NS / G)] = v[q];
+    } else if constexpr (DNS2D_IDX && G % NS == 0 && (NS * R) % G == 0) {
+        float2 *__restrict__ b = y + A + (A >> PS) + k;
 #pragma unroll
-        for (int q = 0; q < R; ++q) b[q * NS + ((q * NS) >> 5)] = v[q];
-    } else if constexpr (DNS2D_IDX && NS == 1 && 32 % R == 0) {
-        float2 *__restrict__ b = y + sidx(A);
+        for (int q = 0; q < R; ++q) b[q * NS + ((q * NS) >> PS)] = v[q];
+    } else if constexpr (DNS2D_IDX && NS == 1 && G % R == 0) {
+        float2 *__restrict__ b = y + sidx<PS>(A);
 #pragma unroll
         for (int q = 0; q < R; ++q) b[q] = v[q];
     } else {
         const int base = A + k;
 #pragma unroll
-        for (int q = 0; q < R; ++q) y[sidx(base + q * NS)] = v[q];
+        for (int q = 0; q < R; ++q) y[sidx<PS>(base + q * NS)] = v[q];
     }
 }
 
@@ -444,7 +448,7 @@ __device__ __forceinline__ constexpr bool slot_in_band(int r)
 }
 
 // last stage (Ns = L/R) with outputs in [B0, B1] dropped
-template <class Cat, int L, int R, bool INV, int B0, int B1>
+template <class Cat, int L, int R, bool INV, int B0, int B1, int PS = 5>
 __device__ __forceinline__ void stage1_last_band(float2 *s, const float2 *tw)
 {
     constexpr int LR = L / R;
@@ -452,20 +456,20 @@ __device__ __forceinline__ void stage1_last_band(float2 *s, const float2 *tw)
     float2 v[R];
     __syncthreads();
     if (j < LR) {
-        sm_load<L, R>(v, s, j);
+        sm_load<L, R, PS>(v, s, j);
         bfly<Cat, L, R, LR, INV>(v, j, tw);
     }
     __syncthreads();
     if (j < LR) {
 #pragma unroll
         for (int q = 0; q < R; ++q)
-            if (!slot_in_band<L, R, B0, B1>(q)) s[sidx(j + q * LR)] = v[q];
+            if (!slot_in_band<L, R, B0, B1>(q)) s[sidx<PS>(j + q * LR)] = v[q];
     }
 }
 
 // smem -> smem stage, one butterfly per thread (threads >= L/R idle); in place, so reads and
 // writes are separated by a barrier.  Leading barrier included; no trailing barrier.
-template <class Cat, int L, int R, int NS, bool INV>
+template <class Cat, int L, int R, int NS, bool INV, int PS = 5>
 __device__ __forceinline__ void stage1(float2 *s, const float2 *tw)
 {
     constexpr int LR = L / R;
@@ -473,11 +477,11 @@ __device__ __forceinline__ void stage1(float2 *s, const float2 *tw)
     float2 v[R];
     __syncthreads();
     if (j < LR) {
-        sm_load<L, R>(v, s, j);
+        sm_load<L, R, PS>(v, s, j);
         bfly<Cat, L, R, NS, INV>(v, j, tw);
     }
     __syncthreads();
-    if (j < LR) sm_store<L, R, NS>(s, v, j);
+    if (j < LR) sm_store<L, R, NS, PS>(s, v, j);
 }
 
 // asynchronous global -> shared copies (cp.async; 8-byte elements, L1-allocating)

@@ -23,6 +23,8 @@ struct KernelSet {
     void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
     void (*rows_fwd_scalar)(const Pointers &, const float *, float2 *, cudaStream_t);
     void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, cudaStream_t);
+    // full 2D R2C of the physical u, w planes (dump path; nullptr at the cluster sizes)
+    void (*velocity_r2c_full)(const Pointers &, const float *, float2 *, cudaStream_t);
 };
 
 template <int N>
@@ -34,7 +36,7 @@ struct Launch {
     static constexpr int GB = C::L / C::ROWS;
 
     static constexpr bool V2 = Cfg2<N>::enabled;
-    static constexpr size_t sm2 = V2 ? (size_t)SmemLen<3 * N / 2>::value * sizeof(float2) : 0;
+    static constexpr size_t sm2 = V2 ? (size_t)Cfg2<N>::LP * sizeof(float2) : 0;
     using P0 = typename C::Plan;
     using P1 = typename AltPlans<N>::P1;
     using P2 = typename AltPlans<N>::P2;
@@ -85,6 +87,8 @@ struct Launch {
         if ((e = cudaFuncSetAttribute(k_rows_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_rows_fwd_scalar<N>, a, (int)smB)) != cudaSuccess) return e;
         if ((e = cudaFuncSetAttribute(k_cols_fwd_scalar<N>, a, (int)smA1)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_rows_r2c_full<N>, a, (int)smB)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_cols_c2c_full<N>, a, (int)smA1)) != cudaSuccess) return e;
         return cudaSuccess;
     }
     static void rows_step(const Pointers &p, cudaStream_t s, int ny)
@@ -138,11 +142,17 @@ struct Launch {
     {
         k_cols_fwd_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, out);
     }
+    static void velocity_r2c_full(const Pointers &p, const float *phys, float2 *spec, cudaStream_t s)
+    {
+        k_rows_r2c_full<N><<<GB, C::NTB, smB, s>>>(p, phys, spec);
+        k_cols_c2c_full<N><<<dim3(C::L / 2 + 1, 2), C::NTA, smA1, s>>>(p, spec);
+    }
     static KernelSet make()
     {
         return KernelSet{N, AltPlans<N>::count, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init,
                          rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar};
+                         rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar,
+                         velocity_r2c_full};
     }
 };
 
@@ -199,7 +209,7 @@ struct LaunchC {
     static KernelSet make()
     {
         return KernelSet{N, 1, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr};
+                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr, nullptr};
     }
 };
 

@@ -22,7 +22,8 @@ ITER_RE = re.compile(r"ITERATION\s+(\d+) T=([-0-9.eE]+) DT=([-0-9.eE]+) CN=([-0-
 
 
 def iterations(text):
-    return {int(m[1]): dict(T=float(m[2]), DT=float(m[3]), CN=float(m[4]), CFLM=float(m[5]), SIG=int(m[9]))
+    return {int(m[1]): dict(T=float(m[2]), DT=float(m[3]), CN=float(m[4]), CFLM=float(m[5]), Re=float(m[6]),
+                            VISC=float(m[7]), PALIN=int(m[8]), SIG=int(m[9]))
             for m in ITER_RE.finditer(text)}
 
 
@@ -283,8 +284,9 @@ def test_c1_thousand_steps_match_reference_cufft(tmp_path):
       against the FP64 scheme).  Its energy history is compared with the oracle run with the same
       float factors (within 2e-6), which isolates that bias; this library's history then lies
       within the FP64-to-float-factor gap plus 2e-6 of the reference's.
-    - Every printed diagnostic: T, DT and CN within the float rounding of the two runs' CFLM, and
-      SIG within one pixel level."""
+    - Every printed diagnostic: DT and CFLM within 3e-5 (each run's CFLM is the maximum over its
+      own field, and the two fields are ~4e-5 apart by step 1000), CN within 2e-6, T within 2e-5
+      (the float sum of the DT sequence), and SIG within one pixel level."""
     N, Re, K0, cfl, steps, update = 512, 1e4, 4.0, 0.1, 1000, 100
     om0 = O.k4_spectrum(N, K0, 0)
     E_ref, Z_ref, diag_ref, om_ref = _ref_harness(N, Re, K0, cfl, steps, update, om0, tmp_path)
@@ -301,10 +303,10 @@ def test_c1_thousand_steps_match_reference_cufft(tmp_path):
     assert sorted(diag) == sorted(diag_ref) == [1] + list(range(100, 1001, 100))
     for it, (t, dt, cn, cflm, sig) in diag_ref.items():
         g = diag[it]
-        assert g[0] == pytest.approx(t, rel=2e-6)
-        assert g[1] == pytest.approx(dt, rel=1e-5)
+        assert g[0] == pytest.approx(t, rel=2e-5)
+        assert g[1] == pytest.approx(dt, rel=3e-5)
         assert g[2] == pytest.approx(cn, abs=2e-6)
-        assert g[3] == pytest.approx(cflm, rel=1e-5)
+        assert g[3] == pytest.approx(cflm, rel=3e-5)
         assert abs(g[4] - sig) <= 1.0
 
 
@@ -333,3 +335,173 @@ def test_cli_matches_reference_binary(args, tmp_path):
         assert o[it]["CFLM"] == pytest.approx(r[it]["CFLM"], rel=1e-5)
         assert abs(o[it]["SIG"] - r[it]["SIG"]) <= 1
 
+
+
+def _spectrum_bins(u, w, nbins):
+    """energy_spectrum.csv bins (cuda/mem_cuda.cu:599-626) of the physical planes u, w, in FP64:
+    forward R2C of each, p = |U|^2 + |W|^2 doubled for 0 < kx < L/2, binned by |k| / (L/2) / sqrt 2."""
+    L = u.shape[0]
+    U, W = np.fft.rfft2(u), np.fft.rfft2(w)
+    p = np.abs(U) ** 2 + np.abs(W) ** 2
+    kx = np.arange(L // 2 + 1)[None, :]
+    z = np.arange(L)[:, None]
+    kz = np.where(z <= L // 2, z, z - L)
+    r = np.sqrt((kx * kx + kz * kz).astype(np.float64)) / (0.5 * L)
+    b = np.clip(np.floor(r / np.sqrt(2.0) * nbins).astype(np.int64), 0, nbins - 1)
+    dbl = (kx > 0) & (kx < L // 2)
+    keep = ~((kx == 0) & (kz == 0))
+    e = np.bincount(b[keep], weights=np.where(dbl, 2 * p, p)[keep], minlength=nbins)
+    c = np.bincount(b[keep], weights=np.broadcast_to(np.where(dbl, 2, 1), b.shape)[keep], minlength=nbins)
+    return e, c.astype(np.int64)
+
+
+def test_energy_spectrum_bins_match_oracle():
+    """The energy_spectrum.csv bins of this library (the forward R2C of the physical velocity over
+    every mode, binned like the reference) against the same binning of the FP64 oracle's velocity
+    after 10 steps: equal counts in every bin; bins with energy above 1e-12 of the total within
+    1e-5 relative (plus a floor of 1e-10 of the total); the bins beyond the retained radius hold
+    only rounding noise, below 1e-9 of the total."""
+    import optimizec_b200 as P
+    N, Re, K0, cfl = 128, 1e4, 4.0, 0.1
+    om0 = O.k4_spectrum(N, K0, 2)
+    s = P.Solver(N, Re, K0, cfl)
+    s.init_vorticity(om0)
+    s.next_dt()
+    s.step(10)
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_om2(om0)
+    o.run_fixed([s.scalars()["dt"]] * 10, [1.0] * 10)
+    nbins = 3 * N
+    e, c = s.velocity_spectrum_bins(nbins)
+    e_o, c_o = _spectrum_bins(o.ur(0), o.ur(1), nbins)
+    o.close()
+    assert np.array_equal(c, c_o)
+    tot = e_o.sum()
+    big = e_o > 1e-12 * tot
+    assert big.sum() > N // 2
+    assert np.all(np.abs(e[big] - e_o[big]) <= 1e-5 * e_o[big] + 1e-10 * tot)
+    assert np.all(e[~big] <= 1e-9 * tot)
+
+
+def _pgm(path):
+    b = open(path, "rb").read()
+    parts = b.split(b"\n", 3)
+    w, h = map(int, parts[1].split())
+    return np.frombuffer(parts[3], dtype=np.uint8).reshape(h, w)
+
+
+def _csv_rows(path):
+    lines = open(path).read().splitlines()
+    return lines[0], [tuple(float(x) for x in l.split(",")) for l in lines[1:]]
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built")
+def test_dump_files_match_reference_binary(tmp_path):
+    """The files of a signal save, against the reference binary's own: the reference runs from a
+    seeded restart.bin and is sent SIGRTMIN, which writes restart.bin and every dump file of the
+    same state into its _restart folder; this CLI's DUMP mode renders that restart.bin.
+    - u_velocity, v_velocity, kinetic, omega (0.1 % / 99.9 % percentile clip), stream PGMs:
+      same header, at most one grey level apart, and at least 99.9 % of the pixels identical (the
+      velocities are rebuilt from the file through this library's transforms, so values sitting on
+      a grey-level boundary can round the other way).
+    - energy_spectrum.csv: the same header and the same rows (bin radius and count), and every
+      energy within 1e-5 relative for bins above 1e-10 of the total; the remaining bins hold the
+      transforms' rounding noise in both files and are compared only for being below that."""
+    N, Re, K0, cfl = 256, 1e4, 4.0, 0.1
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_om2(O.k4_spectrum(N, K0, 4))
+    rb = tmp_path / "start.bin"
+    O.write_restart_v2(str(rb), o, Re, K0, cfl)
+    o.close()
+    run = tmp_path / "ref"
+    run.mkdir()
+    proc = subprocess.Popen([REF, str(N), "10000", "4", "1000000", "0.1", "50", "0", str(rb)], cwd=run,
+                            stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    try:
+        _wait_for(proc, r"ITERATION\s+100 ", timeout=120)
+        proc.send_signal(signal.SIGRTMIN)
+        _wait_for(proc, r"_restart/meta\.csv", timeout=120)
+        proc.send_signal(signal.SIGINT)
+        proc.communicate(timeout=60)
+    finally:
+        if proc.poll() is None:
+            proc.kill()
+    folders = [d for d in os.listdir(run) if d.endswith("_restart")]
+    assert len(folders) == 1, folders
+    ref = run / folders[0]
+    ours = tmp_path / "ours"
+    p = subprocess.run([CLI, "DUMP", str(ref / "restart.bin"), str(ours), "50"], capture_output=True, text=True,
+                       timeout=300)
+    assert p.returncode == 0, p.stderr + p.stdout
+    for f in ["u_velocity.pgm", "v_velocity.pgm", "kinetic.pgm", "omega.pgm", "stream.pgm"]:
+        a, b = _pgm(ours / f), _pgm(ref / f)
+        assert a.shape == b.shape == (3 * N // 2, 3 * N // 2), f
+        d = np.abs(a.astype(np.int64) - b.astype(np.int64))
+        assert d.max() <= 1 and (d == 0).mean() >= 0.999, (f, int(d.max()), float((d == 0).mean()))
+    ha, ra = _csv_rows(ours / "energy_spectrum.csv")
+    hb, rb_ = _csv_rows(ref / "energy_spectrum.csv")
+    assert ha == hb == "normalized_radius,shell_sum_energy,count"
+    assert [(r[0], r[2]) for r in ra] == [(r[0], r[2]) for r in rb_]
+    ea, eb = np.array([r[1] for r in ra]), np.array([r[1] for r in rb_])
+    tot = eb.sum()
+    big = eb > 1e-10 * tot
+    assert np.all(np.abs(ea[big] - eb[big]) <= 1e-5 * eb[big]), np.max(np.abs(ea[big] / eb[big] - 1))
+    assert np.all(ea[~big] <= 1e-9 * tot)
+
+
+def _palin_fp64(om2):
+    """The reference's palinstrophy ratio (cuda/mem_cuda.cu:872-940) in FP64 on [iz][ix] om2:
+    sum w k^2 |om|^2 / ((sum w |om|^2 - |om_00|^2) kmax^2), w = 1 on ix = 0 and ix = N/2 - 1, else 2."""
+    N, H = om2.shape
+    ax = np.arange(H, dtype=np.float64)[None, :]
+    iz = np.arange(N)[:, None]
+    gz = np.where(iz < N // 2, iz, iz - N).astype(np.float64)
+    k2 = ax * ax + gz * gz
+    w = np.where((np.arange(H) == 0) | (np.arange(H) == H - 1), 1.0, 2.0)[None, :]
+    p = np.abs(om2.astype(np.complex128)) ** 2
+    total = float((w * p).sum()) - float(p[0, 0])
+    return float((w * k2 * p).sum()) / (total * float(k2.max()))
+
+
+@pytest.mark.parametrize("N", [64, 512, 2048])
+def test_palin_matches_fp64_formula(N):
+    """dns2d_palin (FP64 reduction on the GPU) against the reference's formula evaluated in FP64 on
+    the host from the same field, after 5 steps of a seeded run: 1e-12 relative."""
+    import optimizec_b200 as P
+    s = P.Solver(N, 1e4, 4.0, 0.1)
+    s.init_vorticity(O.k4_spectrum(N, 4.0, 3))
+    s.next_dt()
+    s.step(5)
+    got = s.palin()
+    want = _palin_fp64(s.om2())
+    s.close()
+    assert got == pytest.approx(want, rel=1e-12)
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built")
+def test_adaptive_viscosity_matches_reference_binary(tmp_path):
+    """ADAPT_VISC=1: both binaries from the same seeded restart.bin (N = 256, 600 steps, UPDATE =
+    20), the PD controller on the filtered palinstrophy ratio moving the viscosity at the diagnostic
+    steps: every printed PALIN within one unit, VISC and Re within 1e-4 relative (printed to 6
+    digits), DT within 1e-5, and the viscosity does change during the run."""
+    N, Re, K0, cfl = 256, 1e4, 4.0, 0.1
+    o = O.Oracle(N, Re, K0, cfl)
+    o.init_om2(O.k4_spectrum(N, K0, 6))
+    rb = tmp_path / "start.bin"
+    O.write_restart_v2(str(rb), o, Re, K0, cfl)
+    o.close()
+    args = [N, 10000, 4, 600, 0.1, 20, 1, str(rb)]
+    (tmp_path / "r").mkdir()
+    (tmp_path / "o").mkdir()
+    ref = run_cli(args, tmp_path / "r", exe=REF)
+    ours = run_cli(args, tmp_path / "o")
+    assert ref.returncode == 0, ref.stderr
+    assert ours.returncode == 0, ours.stderr
+    r, g = iterations(ref.stdout), iterations(ours.stdout)
+    assert sorted(r) == sorted(g) and len(r) == 31
+    for it in r:
+        assert abs(g[it]["PALIN"] - r[it]["PALIN"]) <= 1, it
+        assert g[it]["VISC"] == pytest.approx(r[it]["VISC"], rel=1e-4), it
+        assert g[it]["Re"] == pytest.approx(r[it]["Re"], rel=1e-4), it
+        assert g[it]["DT"] == pytest.approx(r[it]["DT"], rel=1e-5, abs=2e-8), it
+    assert len({r[it]["VISC"] for it in r}) > 1  # the controller acted
