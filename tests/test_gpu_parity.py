@@ -89,7 +89,7 @@ def test_twenty_steps_match_oracle(N, Re):
 def test_pao_start_matches_reference_stdout(golden, name):
     """The reference's own recorded runs (N = 512, 4096 and 16384, PAO-k^-3 start): PAO seed and
     energy, the initial CFLM, then T, DT, CN, CFLM and SIG at every printed iteration (the first
-    1000 steps of the N = 512 run).  Up to step 100: the printed digits, one float ulp of CN and
+    1000 steps of the N = 512 run).  Up to step 100: the printed digits, two float ulps of CN and
     1e-6 relative on CFLM.  Later the two FP32 trajectories (the recording GPU's cuFFT and this
     code) drift apart: CFLM within 2e-5, CN within 5e-6, T within 1e-6 relative, SIG within 1."""
     run = [r for r in golden["runs"] if r["file"].startswith(name + "_")][0]
@@ -112,8 +112,9 @@ def test_pao_start_matches_reference_stdout(golden, name):
         assert sc["dt"] == pytest.approx(g["DT"], abs=1e-8), g["it"]
         if g["it"] <= 100:
             assert sc["t"] == pytest.approx(g["T"], abs=2e-10), g["it"]
-            # CN is printed with 8 decimals; FP32 rounding of CFLM moves it by up to one float ulp
-            assert sc["cn"] == pytest.approx(g["CN"], abs=1.2e-7), g["it"]
+            # CN is printed with 8 decimals; FP32 rounding of CFLM, and the recorded runs' float
+            # Crank-Nicolson factors (see CFLM below), move it by up to two float ulps
+            assert sc["cn"] == pytest.approx(g["CN"], abs=2.4e-7), g["it"]
             # 1e-6: the recorded runs form their Crank-Nicolson factors in float, which biases
             # their viscous decay by ~1e-8 per step against the FP64 factors used here
             assert sc["cflm"] == pytest.approx(g["CFLM"], rel=1e-6), g["it"]
