@@ -378,7 +378,7 @@ def test_energy_spectrum_bins_match_oracle():
     assert np.array_equal(c, c_o)
     tot = e_o.sum()
     big = e_o > 1e-12 * tot
-    assert big.sum() > N // 2
+    assert big.sum() >= 20  # the k^4 field at K0 = 4 fills the low-k shells only
     assert np.all(np.abs(e[big] - e_o[big]) <= 1e-5 * e_o[big] + 1e-10 * tot)
     assert np.all(e[~big] <= 1e-9 * tot)
 
