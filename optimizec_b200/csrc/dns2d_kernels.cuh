@@ -479,29 +479,20 @@ struct TwCat {
     static constexpr int off(int R, int NS) { return cat.find(R, NS); }
 };
 
-// three CTAs per SM: the register allocator keeps the row pass at 56 registers (36 warps per SM;
-// N = 4096: 0.311 -> 0.280 ms against two CTAs at 80 registers)
+// Inverse x transform of a row pair on the large-grid plan: the half spectra A = U[k], B = W[k]
+// (k < H, consecutive k 4 float2 apart, as in the work layout) of two real rows a, b are packed
+// Hermitian-wise as A + iB and transformed (C2R semantics: only Re of the k = 0 entries is used).
+// Thread j < L/R3 is left holding v[q] = (a(x), b(x)) at x = j + q L/R3; the last inverse stage
+// runs in registers.  Used by the row pass (rows u, w of one physical row), NEXTDT (the same,
+// for the CFL maximum) and OM2PHYS (two physical rows of one field).
 template <int N>
-__global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
+__device__ __forceinline__ void rows_inverse2(const float2 *__restrict__ U, const float2 *__restrict__ W, float2 *s,
+                                              const float2 *__restrict__ tw, float2 (&v)[Cfg2<N>::R3])
 {
-    const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
     constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS;
     constexpr int LR1 = L / R1, LR3 = L / R3;
-    extern __shared__ float2 s[];
-    const int z = blockIdx.x;
     const int j = threadIdx.x;
-    const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
-    const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
-    // bring to L2 the quarter (z % 4) of the 4-row tile that the CTA pf_rows later reads (two
-    // waves of 148 SMs x 2 CTAs by default)
-    if (p.pf_rows > 0 && z + p.pf_rows < L) {
-        const int t = (z + p.pf_rows) >> 2, part = z & 3;
-        constexpr int QB = H * 32 / 4;  // bytes of one quarter tile of one component
-        const char *b0 = reinterpret_cast<const char *>(p.work + (size_t)t * H * 4) + part * QB;
-        for (int o = j * 128; o < 2 * QB; o += C::NT * 128)
-            prefetch_l2(o < QB ? b0 + o : b0 + (size_t)L * H * 8 + (o - QB));
-    }
     // inverse stage 1 (Ns = 1), inputs Z[j + r L/R1] of the Hermitian packing of U + iW.  Z at
     // k > L-H needs U, W at L-k = (L/R1 - j) + (R1-1-r) L/R1: slot R1-1-r of butterfly L/R1 - j.
     // Butterflies j and L/R1 - j share a warp 16 lanes apart, so every thread loads only its
@@ -558,13 +549,42 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
         DFT<R1, true>::run(v);
         sm_store<L, R1, 1, PS>(s, v, jb);
     }
-    stage1<TwCat<N>, L, R2, R1, true, PS>(s, p.tw);
-    // inverse stage 3 into registers -> products -> forward stage 1
-    float2 v[R3];
+    stage1<TwCat<N>, L, R2, R1, true, PS>(s, tw);
     __syncthreads();
     if (j < LR3) {
         sm_load<L, R3, PS>(v, s, j);
-        bfly<TwCat<N>, L, R3, LR3, true>(v, j, p.tw);
+        bfly<TwCat<N>, L, R3, LR3, true>(v, j, tw);
+    }
+}
+
+// three CTAs per SM: the register allocator keeps the row pass at 56 registers (36 warps per SM;
+// N = 4096: 0.311 -> 0.280 ms against two CTAs at 80 registers)
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
+{
+    const Pointers p = p0.member(blockIdx.y);
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS;
+    constexpr int LR1 = L / R1, LR3 = L / R3;
+    extern __shared__ float2 s[];
+    const int z = blockIdx.x;
+    const int j = threadIdx.x;
+    const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
+    const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
+    // bring to L2 the quarter (z % 4) of the 4-row tile that the CTA pf_rows later reads (two
+    // waves of 148 SMs x 2 CTAs by default)
+    if (p.pf_rows > 0 && z + p.pf_rows < L) {
+        const int t = (z + p.pf_rows) >> 2, part = z & 3;
+        constexpr int QB = H * 32 / 4;  // bytes of one quarter tile of one component
+        const char *b0 = reinterpret_cast<const char *>(p.work + (size_t)t * H * 4) + part * QB;
+        for (int o = j * 128; o < 2 * QB; o += C::NT * 128)
+            prefetch_l2(o < QB ? b0 + o : b0 + (size_t)L * H * 8 + (o - QB));
+    }
+    // inverse x transform; its last stage leaves u + i w in registers -> products -> forward
+    // stage 1
+    float2 v[R3];
+    rows_inverse2<N>(U, W, s, p.tw, v);
+    if (j < LR3) {
 #pragma unroll
         for (int q = 0; q < R3; ++q) v[q] = make_float2(v[q].x * v[q].x - v[q].y * v[q].y, 2.0f * v[q].x * v[q].y);
         DFT<R3, false>::run(v);
@@ -892,6 +912,109 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
 #pragma unroll
         for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// Diagnostics on the large-grid plans (the sizes with Cfg2): NEXTDT's CFL maximum and the
+// physical velocity planes (as k_rows_velocity), and OM2PHYS / the stream function (as
+// k_cols_scalar + k_rows_scalar), on the step kernels' transforms.
+// ------------------------------------------------------------------------------------------
+// one physical row: u, w into phys[0..1] (when phys != nullptr) and the CFL maximum
+// max |u|/dx + |w|/dx (cuda/dns_cuda.cu:486-522) into cflm (when cflm != nullptr)
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_velocity2(Pointers p0, float *phys, float *cflm, float dx)
+{
+    const Pointers p = p0.member(blockIdx.y);
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, R3 = C::R3, LR3 = L / R3, NT = C::NT;
+    extern __shared__ float2 s[];
+    __shared__ float red[32];
+    const int z = blockIdx.x, j = threadIdx.x;
+    float2 v[R3];
+    rows_inverse2<N>(p.work + widx<L, H>(0, z, 0), p.work + widx<L, H>(1, z, 0), s, p.tw, v);
+    float m = 0.0f;
+    if (j < LR3) {
+#pragma unroll
+        for (int q = 0; q < R3; ++q) {
+            if (phys) {
+                const size_t o = (size_t)z * L + j + q * LR3;
+                phys[o] = v[q].x;
+                phys[(size_t)L * L + o] = v[q].y;
+            }
+            m = fmaxf(m, cfl_term(v[q].x, v[q].y, dx));
+        }
+    }
+    if (cflm) {
+        m = block_max<NT>(m, red);
+        if (threadIdx.x == 0) atomic_max_nonneg(cflm + blockIdx.y, m);
+    }
+}
+
+// one column: om2 (kind 0) or the stream function om2 / K^2 (kind 1; 0 at k = 0) -> inverse z
+// transform -> scratch component 0 in the work layout
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT) k_cols_scalar2(Pointers p, float2 *scratch, int kind)
+{
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, NT = C::NT, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS, LR1 = L / R1;
+    extern __shared__ float2 s[];
+    const int kx = blockIdx.x, j = threadIdx.x;
+    for (int iz = j; iz < N; iz += NT) {
+        const int kz = (iz < H) ? iz : iz - N;
+        const int kzi = (kz >= 0) ? kz : kz + L;
+        float2 v = p.om2[(size_t)kx * N + iz];
+        if (kind == 1) {
+            const float k2 = (float)kx * (float)kx + (float)kz * (float)kz + 1.0e-30f;
+            v = make_float2(v.x / k2, v.y / k2);
+            if (kx == 0 && iz == 0) v = make_float2(0.f, 0.f);
+        }
+        s[sidx<PS>(kzi)] = v;
+    }
+    for (int z = H + j; z < L - H; z += NT)
+        if (!slot_in_band<L, R3, H, L - H - 1>(z / (L / R3))) s[sidx<PS>(z)] = make_float2(0.f, 0.f);
+    stage1g_first_band<TwCat<N>, L, R3, true, NT, H, L - H - 1, PS>(s, p.tw, j, 1);
+    stage1g<TwCat<N>, L, R2, R3, true, NT, PS>(s, p.tw, j, 1);
+    group_sync<NT>(1);
+    if (j < LR1) {
+        float2 v[R1];
+        sm_load<L, R1, PS>(v, s, j);
+        bfly<TwCat<N>, L, R1, LR1, true>(v, j, p.tw);
+        constexpr size_t QS = (size_t)(LR1 / 4) * H * 4;
+        float2 *ptr = scratch + widx<L, H>(0, j, kx);
+#pragma unroll
+        for (int q = 0; q < R1; ++q, ptr += QS) *ptr = v[q];
+    }
+}
+
+// two physical rows z = 2 blockIdx.x, z + 1 of a real field from its x half spectra (scratch
+// component 0) -> out, with the CTA's min / max into minmax[blockIdx.x]
+template <int N>
+__global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_pair2(Pointers p, const float2 *scratch, float *out,
+                                                             float2 *minmax)
+{
+    using C = Cfg2<N>;
+    constexpr int L = C::L, H = C::H, R3 = C::R3, LR3 = L / R3, NT = C::NT;
+    extern __shared__ float2 s[];
+    __shared__ float red[32];
+    const int z = 2 * blockIdx.x, j = threadIdx.x;
+    float2 v[R3];
+    rows_inverse2<N>(scratch + widx<L, H>(0, z, 0), scratch + widx<L, H>(0, z + 1, 0), s, p.tw, v);
+    float mn = 3.402823466e38f, mx = -3.402823466e38f;
+    if (j < LR3) {
+#pragma unroll
+        for (int q = 0; q < R3; ++q) {
+            const size_t o = (size_t)z * L + j + q * LR3;
+            out[o] = v[q].x;
+            out[o + L] = v[q].y;
+            mn = fminf(mn, fminf(v[q].x, v[q].y));
+            mx = fmaxf(mx, fmaxf(v[q].x, v[q].y));
+        }
+    }
+    __shared__ float s_nmn;
+    const float nmn = block_max<NT>(-mn, red);
+    if (threadIdx.x == 0) s_nmn = nmn;
+    const float bmx = block_max<NT>(mx, red);
+    if (threadIdx.x == 0) minmax[blockIdx.x] = make_float2(-s_nmn, bmx);
 }
 
 // ------------------------------------------------------------------------------------------

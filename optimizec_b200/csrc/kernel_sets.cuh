@@ -73,6 +73,9 @@ struct Launch {
             if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_rows_velocity2<N>, a, (int)sm2)) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_cols_scalar2<N>, a, (int)sm2)) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_rows_pair2<N>, a, (int)sm2)) != cudaSuccess) return e;
         }
         if constexpr (!V2) {  // rows per CTA x radix plan variants of the small-grid passes
             if ((e = setup_plan<P0>()) != cudaSuccess) return e;
@@ -118,9 +121,11 @@ struct Launch {
     {
         k_cols_init<N><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, uw, mode);
     }
+    // the diagnostics of the large-grid sizes run on the step kernels' plan (Cfg2)
     static void rows_velocity(const Pointers &p, float *phys, float *cflm, float dx, cudaStream_t s, int ny)
     {
-        k_rows_velocity<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p, phys, cflm, dx);
+        if constexpr (V2) k_rows_velocity2<N><<<dim3(C::L, ny), Cfg2<N>::NT, sm2, s>>>(p, phys, cflm, dx);
+        else k_rows_velocity<N><<<dim3(GB, ny), C::NTB, smB, s>>>(p, phys, cflm, dx);
     }
     static void rows_from_phys(const Pointers &p, const float *phys, cudaStream_t s)
     {
@@ -128,11 +133,14 @@ struct Launch {
     }
     static void cols_scalar(const Pointers &p, float2 *scratch, int kind, cudaStream_t s)
     {
-        k_cols_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, kind);
+        if constexpr (V2) k_cols_scalar2<N><<<C::H, Cfg2<N>::NT, sm2, s>>>(p, scratch, kind);
+        else k_cols_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, kind);
     }
+    // one min / max pair per CTA into mm: GB of them, or L / 2 on the large-grid plan
     static void rows_scalar(const Pointers &p, const float2 *scratch, float *out, float2 *mm, cudaStream_t s)
     {
-        k_rows_scalar<N><<<GB, C::NTB, smB, s>>>(p, scratch, out, mm);
+        if constexpr (V2) k_rows_pair2<N><<<C::L / 2, Cfg2<N>::NT, sm2, s>>>(p, scratch, out, mm);
+        else k_rows_scalar<N><<<GB, C::NTB, smB, s>>>(p, scratch, out, mm);
     }
     static void rows_fwd_scalar(const Pointers &p, const float *f, float2 *scratch, cudaStream_t s)
     {
@@ -149,7 +157,8 @@ struct Launch {
     }
     static KernelSet make()
     {
-        return KernelSet{N, AltPlans<N>::count, GB, &TwCat<N>::cat, setup, rows_step, cols_step, cols_init,
+        return KernelSet{N, AltPlans<N>::count, V2 ? std::max(GB, C::L / 2) : GB, &TwCat<N>::cat, setup, rows_step,
+                         cols_step, cols_init,
                          rows_velocity,
                          rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar,
                          velocity_r2c_full};

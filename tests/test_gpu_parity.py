@@ -34,7 +34,7 @@ def _run_pair(N, K0, Re, cfl, steps, update, seed=0):
     return o, s, c
 
 
-@pytest.mark.parametrize("N", [16, 32, 64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("N", [16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
 def test_initial_velocity_matches_oracle(N):
     o, s, cflm = _run_pair(N, 4.0, 1e4, 0.1, 0, 100)
     s.velocity_phys()
@@ -126,14 +126,32 @@ def test_pao_start_matches_reference_stdout(golden, name):
             assert abs(int(sig) - g["SIG"]) <= 1, g["it"]
 
 
-def test_omega_phys_and_sigma_match_oracle():
-    N = 256
+@pytest.mark.parametrize("N", [256, 1024, 2048, 4096])
+def test_omega_phys_and_sigma_match_oracle(N):
+    """OM2PHYS and the display sigma (N >= 1024: on the step kernels' plan, two physical rows per
+    complex transform) and the stream function against the oracle's FP64 field."""
     o, s, _ = _run_pair(N, 4.0, 1e4, 0.1, 0, 100, seed=3)
     s.om2phys()
     w_gpu = s.phys(2).astype(np.float64)
     w_ref = o.omega_phys()
     assert rel_l2(w_gpu, w_ref) < 2e-6
     assert int(s.display_sigma(2)) == int(O.display_sigma(w_ref))
+    # stream function: psi = inverse transform of om2 / K^2 (0 at k = 0)
+    s.stream_func()
+    psi = s.phys(2).astype(np.float64)
+    om = o.om2()
+    H = N // 2
+    kz = np.where(np.arange(N) < H, np.arange(N), np.arange(N) - N)[:, None].astype(np.float64)
+    k2 = np.arange(H)[None, :] ** 2 + kz ** 2
+    k2[0, 0] = 1.0
+    ps = om / k2
+    ps[0, 0] = 0.0
+    L = 3 * N // 2
+    full = np.zeros((L, L // 2 + 1), dtype=np.complex128)
+    full[:H, :H] = ps[:H]
+    full[L - H:, :H] = ps[H:]
+    psi_ref = O.inv2d(full)
+    assert rel_l2(psi, psi_ref) < 2e-6
 
 
 def test_restart_roundtrip(tmp_path):
