@@ -185,6 +185,22 @@ int dns2d_batch_next_dt(dns2d_batch *b, float *cflm);
 int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, double *Z_hist);
 /* build the graphs a later dns2d_batch_step(b, nsteps) launches, without running them */
 int dns2d_batch_prepare(dns2d_batch *b, int nsteps);
+/* Stepping mode of a batch (no counterpart in the reference): 0 = one CUDA graph per chunk of up
+ * to 128 steps, each size group's row and column kernels a parallel branch (default); 1 = one
+ * persistent launch per chunk: every member of every size advances inside one cooperative kernel
+ * whose CTAs take row and column work items in dependency order and wait on per-member
+ * completion counters (sizes 64, 128, 256, 512, each on its default radix plan; the fields equal
+ * mode 0's on those plans bit for bit).  DNS2D_ERR_SIZE when the batch holds another size. */
+int dns2d_batch_set_mode(dns2d_batch *b, int mode);
+/* The persistent launch's dependency waits: polls of a counter before a wait gives up, which
+ * makes dns2d_batch_step return DNS2D_ERR_TIMEOUT with the context still usable (default 4 M,
+ * about a second), and a member whose column items wait for a count that nothing reaches (-1:
+ * none), with which a test makes a wait run out. */
+int dns2d_batch_set_waits(dns2d_batch *b, long long spin_limit, int stall_member);
+/* Work-item size of the persistent launch (powers of two up to 64, reduced per size group to a
+ * divisor of its count): row tiles of 4 physical rows per row item (default 8) and column groups
+ * per column item (default 4).  Scheduling only: the results do not change. */
+int dns2d_batch_set_items(dns2d_batch *b, int tiles_per_item, int groups_per_item);
 int dns2d_batch_sync(dns2d_batch *b);
 int dns2d_batch_get_om2(dns2d_batch *b, int member, float *om2);
 int dns2d_batch_get_scalars(dns2d_batch *b, int member, dns2d_scalars *out);

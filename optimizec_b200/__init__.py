@@ -43,12 +43,13 @@ SYMBOLS = [
     "dns2d_cnn_get_params", "dns2d_cnn_set_params", "dns2d_cnn_forward", "dns2d_cnn_loss_grad",
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
-    "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare", "dns2d_batch_prepare",
+    "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare", "dns2d_batch_prepare", "dns2d_batch_set_mode",
+    "dns2d_batch_set_waits", "dns2d_batch_set_items",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # translation units of libdns2d.so: the C ABI and one unit per group of compiled grid sizes
-SOURCES = ["dns2d_api.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
+SOURCES = ["dns2d_api.cu", "ensemble.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
            "sets_29400.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]
@@ -183,6 +184,9 @@ def lib():
         "dns2d_movie_scale": (C.c_int, [C.c_int]),
         "dns2d_prepare": (C.c_int, [vp, C.c_int]),
         "dns2d_batch_prepare": (C.c_int, [vp, C.c_int]),
+        "dns2d_batch_set_mode": (C.c_int, [vp, C.c_int]),
+        "dns2d_batch_set_waits": (C.c_int, [vp, C.c_longlong, C.c_int]),
+        "dns2d_batch_set_items": (C.c_int, [vp, C.c_int, C.c_int]),
         "dns2d_movie_frame": (C.c_int, [vp, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_double)]),
     }
@@ -475,6 +479,19 @@ class Batch:
     def autotune(self):
         """Time each size group's kernel variants at its member count (before init_k4)."""
         self._chk(self._L.dns2d_batch_autotune(self._b))
+
+    def set_mode(self, mode: int):
+        """0: one CUDA graph per chunk, a branch per size group; 1: one persistent launch per
+        chunk (dns2d_batch_set_mode)."""
+        self._chk(self._L.dns2d_batch_set_mode(self._b, int(mode)))
+
+    def set_items(self, tiles_per_item: int, groups_per_item: int):
+        """Work-item size of the persistent launch (dns2d_batch_set_items)."""
+        self._chk(self._L.dns2d_batch_set_items(self._b, int(tiles_per_item), int(groups_per_item)))
+
+    def set_waits(self, spin_limit: int, stall_member: int = -1):
+        """Dependency waits of the persistent launch (dns2d_batch_set_waits)."""
+        self._chk(self._L.dns2d_batch_set_waits(self._b, int(spin_limit), int(stall_member)))
 
     def prepare(self, n: int):
         """Build the graphs step(n) will launch, without running them (dns2d_batch_prepare)."""

@@ -15,6 +15,7 @@
 // The kernels of the passes are in dns2d_kernels.cuh / cluster.cuh, their launch tables in
 // kernel_sets.cuh (instantiated by sets_*.cu).
 #include "kernel_sets.cuh"
+#include "ensemble.cuh"
 #include "cnn.cuh"
 #include "cnn_tc.cuh"
 #include "../../include/dns2d.h"
@@ -162,8 +163,8 @@ __global__ void k_minmax(const float *f, size_t n, float2 *out)
 }
 
 // 8-bit display quantisation sums (cuda/mem_cuda.cu:691-740): same IEEE operation sequence
-__global__ void k_sigma_pixels(const float *f, size_t n, float minv, float rng, int is_constant,
-                               unsigned long long *sums)
+__device__ __forceinline__ void sigma_pixel_sums(const float *f, size_t n, float minv, float rng, int is_constant,
+                                                 unsigned long long *sums)
 {
     __shared__ unsigned long long s1[256], s2[256];
     unsigned long long a = 0, b = 0;
@@ -193,6 +194,38 @@ __global__ void k_sigma_pixels(const float *f, size_t n, float minv, float rng, 
         sums[2 * blockIdx.x] = s1[0];
         sums[2 * blockIdx.x + 1] = s2[0];
     }
+}
+
+__global__ void k_sigma_pixels(const float *f, size_t n, float minv, float rng, int is_constant,
+                               unsigned long long *sums)
+{
+    sigma_pixel_sums(f, n, minv, rng, is_constant, sums);
+}
+
+// the same from min / max partials already on the device (every block reduces them itself, in
+// float like the host: min / max are exact, so the result equals a separate min / max pass)
+__global__ void k_sigma_pixels_mm(const float *f, size_t n, const float2 *mm, int nparts, unsigned long long *sums)
+{
+    __shared__ float smn[256], smx[256];
+    float mn = 3.402823466e38f, mx = -3.402823466e38f;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        const float2 q = mm[i];
+        mn = fminf(mn, q.x);
+        mx = fmaxf(mx, q.y);
+    }
+    smn[threadIdx.x] = mn;
+    smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            smn[threadIdx.x] = fminf(smn[threadIdx.x], smn[threadIdx.x + o]);
+            smx[threadIdx.x] = fmaxf(smx[threadIdx.x], smx[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    const float minv = smn[0], maxv = smx[0];
+    const float rng = __fsub_rn(maxv, minv);
+    sigma_pixel_sums(f, n, minv, rng, fabsf(rng) <= 1.0e-12f ? 1 : 0, sums);
 }
 
 // FP64 reductions over the [kx][kz] vorticity: out[block] = {E, Z, pal, total_full, k00, kmax2}
@@ -318,6 +351,9 @@ struct dns2d_state {
     // device buffers
     float2 *om2 = nullptr, *fnm1 = nullptr, *work = nullptr, *tw = nullptr, *scratch = nullptr;
     float *phys = nullptr;
+    // min/max partials of phys plane 2 in `minmax` left by OM2PHYS / the stream function (0: none
+    // valid); display_sigma of plane 2 then needs no min/max pass of its own
+    int mm_plane2 = 0;
     StepParams *prm = nullptr;
     double2 *part = nullptr, *hist = nullptr;
     unsigned int *counter = nullptr;
@@ -811,6 +847,7 @@ extern "C" int dns2d_init_pao(dns2d_state *s, double *stats19, int *pao_seed)
     // the compact velocity spectrum (2 N^2/2 complex) is staged in the phys buffer
     if (bytes > 3 * (size_t)s->L * s->L * 4) return fail(s, DNS2D_ERR_NOMEM, "PAO staging");
     d_uw = reinterpret_cast<float2 *>(s->phys);
+    s->mm_plane2 = 0;
     DNS2D_CUDA(cudaMemcpyAsync(d_uw, uw.data(), bytes, cudaMemcpyHostToDevice, s->stream), "PAO upload");
     s->ks->cols_init(s->ptrs(), d_uw, 0, s->stream, 1);
     DNS2D_LAUNCHED("cols_init(PAO)");
@@ -1208,6 +1245,7 @@ extern "C" int dns2d_movie_frame(dns2d_state *s, int comp, int scale_f, unsigned
     const float *f = s->phys + (size_t)comp * plane;
     const int nb = (int)std::min<size_t>(kFrameBlocks, std::max<size_t>(1, (plane + 255) / 256));
     static_assert(kFrameBlocks <= kSigmaBlocks, "frame partials share the sigma buffers");
+    s->mm_plane2 = 0;
     k_frame_minmax<<<nb, 256, 0, s->stream>>>(f, plane, s->minmax);
     DNS2D_LAUNCHED("frame minmax");
     std::vector<float2> mm((size_t)nb);
@@ -1268,6 +1306,7 @@ extern "C" int dns2d_om2phys(dns2d_state *s)
     DNS2D_LAUNCHED("cols_scalar");
     s->ks->rows_scalar(s->ptrs(), s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
     DNS2D_LAUNCHED("rows_scalar");
+    s->mm_plane2 = s->ks->scalar_parts;
     phase_end(s, 3);
     return DNS2D_OK;
 }
@@ -1280,6 +1319,7 @@ extern "C" int dns2d_stream_func(dns2d_state *s)
     DNS2D_LAUNCHED("cols_scalar(psi)");
     s->ks->rows_scalar(s->ptrs(), s->scratch, s->phys + 2 * plane, s->minmax, s->stream);
     DNS2D_LAUNCHED("rows_scalar(psi)");
+    s->mm_plane2 = s->ks->scalar_parts;
     return DNS2D_OK;
 }
 
@@ -1296,10 +1336,31 @@ extern "C" int dns2d_kinetic(dns2d_state *s)
 {
     if (!s) return DNS2D_ERR_ARG;
     const size_t plane = (size_t)s->L * s->L;
+    s->mm_plane2 = 0;
     k_kinetic<<<1024, 256, 0, s->stream>>>(s->phys, plane);
     DNS2D_LAUNCHED("kinetic");
     return DNS2D_OK;
 }
+
+namespace {
+// sigma = sqrt(E[pix^2] - E[pix]^2) from the per-block pixel sums (integers: exact)
+int sigma_finish(dns2d_state *s, int nb, size_t plane, double *sigma)
+{
+    std::vector<unsigned long long> hs((size_t)nb * 2);
+    DNS2D_CUDA(cudaMemcpyAsync(hs.data(), s->sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, s->stream), "sums copy");
+    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "sums sync");
+    unsigned long long a = 0, b = 0;
+    for (int i = 0; i < nb; ++i) {
+        a += hs[2 * (size_t)i];
+        b += hs[2 * (size_t)i + 1];
+    }
+    const double mean = (double)a / (double)plane;
+    const double var = std::max(0.0, (double)b / (double)plane - mean * mean);
+    *sigma = std::sqrt(var);
+    phase_end(s, 3);
+    return DNS2D_OK;
+}
+}  // namespace
 
 extern "C" int dns2d_display_sigma(dns2d_state *s, int comp, double *sigma)
 {
@@ -1308,6 +1369,12 @@ extern "C" int dns2d_display_sigma(dns2d_state *s, int comp, double *sigma)
     const size_t plane = (size_t)s->L * s->L;
     const float *f = s->phys + (size_t)comp * plane;
     const int nb = (int)std::min<size_t>(kSigmaBlocks, std::max<size_t>(1, (plane + 255) / 256));
+    if (comp == 2 && s->mm_plane2 > 0) {  // min / max partials of this plane from OM2PHYS
+        k_sigma_pixels_mm<<<nb, 256, 0, s->stream>>>(f, plane, s->minmax, s->mm_plane2, s->sums);
+        DNS2D_LAUNCHED("sigma pixels");
+        return sigma_finish(s, nb, plane, sigma);
+    }
+    s->mm_plane2 = 0;
     k_minmax<<<nb, 256, 0, s->stream>>>(f, plane, s->minmax);
     DNS2D_LAUNCHED("minmax");
     std::vector<float2> mm((size_t)nb);
@@ -1322,19 +1389,7 @@ extern "C" int dns2d_display_sigma(dns2d_state *s, int comp, double *sigma)
     const int is_constant = (std::fabs(rng) <= 1.0e-12f) ? 1 : 0;
     k_sigma_pixels<<<nb, 256, 0, s->stream>>>(f, plane, minv, rng, is_constant, s->sums);
     DNS2D_LAUNCHED("sigma pixels");
-    std::vector<unsigned long long> hs((size_t)nb * 2);
-    DNS2D_CUDA(cudaMemcpyAsync(hs.data(), s->sums, (size_t)nb * 16, cudaMemcpyDeviceToHost, s->stream), "sums copy");
-    DNS2D_CUDA(cudaStreamSynchronize(s->stream), "sums sync");
-    unsigned long long a = 0, b = 0;
-    for (int i = 0; i < nb; ++i) {
-        a += hs[2 * (size_t)i];
-        b += hs[2 * (size_t)i + 1];
-    }
-    const double mean = (double)a / (double)plane;
-    const double var = std::max(0.0, (double)b / (double)plane - mean * mean);
-    *sigma = std::sqrt(var);
-    phase_end(s, 3);
-    return DNS2D_OK;
+    return sigma_finish(s, nb, plane, sigma);
 }
 
 namespace {
@@ -1717,6 +1772,7 @@ extern "C" int dns2d_save_restart(dns2d_state *s, const char *path)
 extern "C" int dns2d_load_restart(dns2d_state *s, const char *path)
 {
     if (!s || !path) return DNS2D_ERR_ARG;
+    s->mm_plane2 = 0;  // the file's UR planes replace the physical planes
     const int fd = ::open(path, O_RDONLY);
     if (fd < 0) return fail(s, DNS2D_ERR_IO, "cannot open %s", path);
     RestartV2 h;
@@ -1900,6 +1956,15 @@ struct dns2d_batch {
     std::vector<cudaEvent_t> joins;
     cudaEvent_t fork = nullptr;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+    // stepping mode: 0 = one CUDA graph per chunk with each size group's row / column kernels as
+    // a branch; 1 = one persistent launch per chunk (ensemble.cuh)
+    int mode = 0;
+    unsigned int *ens = nullptr;  // persistent launch: ticket, rows_done[count], cols_done[count], status
+    int *ens_status_host = nullptr;
+    long long spin_limit = 1ll << 22;  // polls of a dependency counter (~1 s) before a wait gives up
+    int stall_member = -1;
+    int ens_grid = 0;
+    int tiles_per_item = 8, groups_per_item = 4;  // persistent launch work-item size (powers of two)
     bool initialised = false;
     std::string err;
 };
@@ -1941,6 +2006,8 @@ extern "C" void dns2d_batch_destroy(dns2d_batch *b)
         cudaFree(g.counter);
         cudaFree(g.cflm);
     }
+    cudaFree(b->ens);
+    if (b->ens_status_host) cudaFreeHost(b->ens_status_host);
     if (b->prm_host) cudaFreeHost(b->prm_host);
     if (b->hist_host) cudaFreeHost(b->hist_host);
     if (b->cflm_host) cudaFreeHost(b->cflm_host);
@@ -2018,7 +2085,9 @@ extern "C" int dns2d_batch_create(dns2d_batch **out, const dns2d_member *members
     }
     if (cudaMallocHost((void **)&b->prm_host, (size_t)count * sizeof(StepParams)) != cudaSuccess ||
         cudaMallocHost((void **)&b->hist_host, (size_t)count * kChunk * 16) != cudaSuccess ||
-        cudaMallocHost((void **)&b->cflm_host, (size_t)count * 4) != cudaSuccess)
+        cudaMallocHost((void **)&b->cflm_host, (size_t)count * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&b->ens_status_host, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&b->ens, (size_t)(2 + 2 * count) * 4) != cudaSuccess)
         return bail(DNS2D_ERR_NOMEM);
     if (b->groups.size() > 1) {
         if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return bail(DNS2D_ERR_CUDA);
@@ -2233,6 +2302,95 @@ int batch_graph(dns2d_batch *b, int first, int K, cudaGraphExec_t *out)
 
 }  // namespace
 
+namespace {
+
+int ens_cols_per_item_of(int N)
+{
+    switch (N) {
+    case 64: return ens_cols_per_item<64>();
+    case 128: return ens_cols_per_item<128>();
+    case 256: return ens_cols_per_item<256>();
+    default: return ens_cols_per_item<512>();
+    }
+}
+
+bool ens_batch_supported(const dns2d_batch *b)
+{
+    if (b->groups.size() > (size_t)kEnsMaxGroups) return false;
+    for (const BatchGroup &g : b->groups)
+        if (!ens_supported(g.N)) return false;
+    return true;
+}
+
+// K steps of every member in one persistent launch (first: the chunk opens a dns2d_batch_step call)
+int ens_chunk(dns2d_batch *b, int first, int K)
+{
+    EnsLaunch q;
+    q.ngroups = (int)b->groups.size();
+    q.steps = K;
+    q.first = first;
+    int member = 0;
+    for (size_t i = 0; i < b->groups.size(); ++i) {
+        const BatchGroup &g = b->groups[i];
+        EnsGroupDev &d = q.g[i];
+        d.N = g.N;
+        d.count = g.count;
+        d.member0 = member;
+        // a few row tiles / column groups per item, so the per-item ticket, wait and completion
+        // count are spread over more work (the items of the small sizes are tiny)
+        const int tiles = g.L / kEnsRows, groups = g.H / ens_cols_per_item_of(g.N);
+        d.tiles_per_item = b->tiles_per_item;
+        while (tiles % d.tiles_per_item) d.tiles_per_item /= 2;
+        d.groups_per_item = b->groups_per_item;
+        while (groups % d.groups_per_item) d.groups_per_item /= 2;
+        d.row_items = tiles / d.tiles_per_item;
+        d.col_items = groups / d.groups_per_item;
+        d.row_begin = q.rows_per_step;
+        d.col_begin = q.cols_per_step;
+        d.p = g.ptrs();
+        q.rows_per_step += g.count * d.row_items;
+        q.cols_per_step += g.count * d.col_items;
+        member += g.count;
+    }
+    q.ticket = b->ens;
+    q.rows_done = b->ens + 1;
+    q.cols_done = b->ens + 1 + b->count;
+    q.status = reinterpret_cast<int *>(b->ens + 1 + 2 * b->count);
+    q.spin_limit = b->spin_limit;
+    q.stall_member = b->stall_member;
+    BATCH_CUDA(cudaMemsetAsync(b->ens, 0, (size_t)(2 + 2 * b->count) * 4, b->stream), "counter reset");
+    BATCH_CUDA(ens_launch(q, b->stream, &b->ens_grid), "persistent ensemble launch");
+    return DNS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int dns2d_batch_set_mode(dns2d_batch *b, int mode)
+{
+    if (!b || mode < 0 || mode > 1) return DNS2D_ERR_ARG;
+    if (mode == 1 && !ens_batch_supported(b))
+        return bfail(b, DNS2D_ERR_SIZE, "persistent launch: sizes 64, 128, 256, 512 and at most 8 size groups");
+    b->mode = mode;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_set_items(dns2d_batch *b, int tiles_per_item, int groups_per_item)
+{
+    auto pow2 = [](int v) { return v >= 1 && v <= 64 && (v & (v - 1)) == 0; };
+    if (!b || !pow2(tiles_per_item) || !pow2(groups_per_item)) return DNS2D_ERR_ARG;
+    b->tiles_per_item = tiles_per_item;
+    b->groups_per_item = groups_per_item;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_batch_set_waits(dns2d_batch *b, long long spin_limit, int stall_member)
+{
+    if (!b || spin_limit < 1 || stall_member >= b->count) return DNS2D_ERR_ARG;
+    b->spin_limit = spin_limit;
+    b->stall_member = stall_member;
+    return DNS2D_OK;
+}
+
 extern "C" int dns2d_batch_prepare(dns2d_batch *b, int nsteps)
 {
     if (!b || nsteps < 0) return DNS2D_ERR_ARG;
@@ -2268,10 +2426,24 @@ extern "C" int dns2d_batch_step(dns2d_batch *b, int nsteps, double *E_hist, doub
     while (done < nsteps) {
         const int K = std::min(kChunk, nsteps - done);
         const int first = (done == 0) ? 1 : 0;
-        cudaGraphExec_t ex = nullptr;
-        const int rc = batch_graph(b, first, K, &ex);
-        if (rc) return rc;
-        BATCH_CUDA(cudaGraphLaunch(ex, b->stream), "graph launch");
+        if (b->mode == 1) {
+            const int rc = ens_chunk(b, first, K);
+            if (rc) return rc;
+        } else {
+            cudaGraphExec_t ex = nullptr;
+            const int rc = batch_graph(b, first, K, &ex);
+            if (rc) return rc;
+            BATCH_CUDA(cudaGraphLaunch(ex, b->stream), "graph launch");
+        }
+        if (b->mode == 1) {
+            // the launch's status: a dependency wait that ran out stops every CTA
+            BATCH_CUDA(cudaMemcpyAsync(b->ens_status_host, b->ens + 1 + 2 * b->count, sizeof(int),
+                                       cudaMemcpyDeviceToHost, b->stream),
+                       "status copy");
+            BATCH_CUDA(cudaStreamSynchronize(b->stream), "status sync");
+            if (*b->ens_status_host != 0)
+                return bfail(b, DNS2D_ERR_TIMEOUT, "persistent ensemble launch: a dependency wait ran out");
+        }
         if (E_hist || Z_hist) {
             off = 0;
             for (BatchGroup &g : b->groups) {
@@ -3022,6 +3194,7 @@ int closure_forcing(dns2d_state *s)
 // one closed step on the device: forcing, energy gate, row pass, column pass (capturable)
 static int closure_device_step(dns2d_state *s, int first, int slot)
 {
+    s->mm_plane2 = 0;  // the closure's inputs are staged in the physical planes
     int rc = closure_forcing(s);
     if (rc) return rc;
     Pointers p = s->ptrs();

@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(Cfg2<N>::NT, 3) k_rows_step2(Pointers p0)
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg2<N>;
     constexpr int L = C::L, H = C::H, R1 = C::R1, R2 = C::R2, R3 = C::R3, PS = C::PS;
-    constexpr int LR1 = L / R1, LR3 = L / R3;
+    constexpr int LR3 = L / R3;
     extern __shared__ float2 s[];
     const int z = blockIdx.x;
     const int j = threadIdx.x;

@@ -313,17 +313,29 @@ struct TwCatalog {
     }
 };
 
-// One Stockham stage over B arrays of length L (array b at s + b*LP).
-template <class Cat, int L, int LP, int R, int NS, bool INV, int B, int NT>
+// The thread index read so that the compiler cannot treat it as loop-invariant: inside a
+// persistent kernel's work loop, expressions of threadIdx.x would otherwise be hoisted out of
+// the loop for every stage of every transform and kept live across it (register spills).
+__device__ __forceinline__ int opaque_tid()
+{
+    int t;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
+    return t;
+}
+
+// One Stockham stage over B arrays of length L (array b at s + b*LP); OPQ: read the thread
+// index with opaque_tid().
+template <class Cat, int L, int LP, int R, int NS, bool INV, int B, int NT, bool OPQ = false>
 __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *__restrict__ tw)
 {
+    const int tid = OPQ ? opaque_tid() : (int)threadIdx.x;
     constexpr int LR = L / R;
     constexpr int TOT = B * LR;
     constexpr int NBF = (TOT + NT - 1) / NT;
     float2 v[NBF][R];
 #pragma unroll
     for (int i = 0; i < NBF; ++i) {
-        const int t = (int)threadIdx.x + i * NT;
+        const int t = tid + i * NT;
         if ((NBF * NT == TOT) || t < TOT) {
             const int b = t / LR;
             const int j = t - b * LR;
@@ -347,7 +359,7 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < NBF; ++i) {
-        const int t = (int)threadIdx.x + i * NT;
+        const int t = tid + i * NT;
         if ((NBF * NT == TOT) || t < TOT) {
             const int b = t / LR;
             const int j = t - b * LR;
@@ -498,18 +510,18 @@ __device__ __forceinline__ void cp_async_wait()
 }
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-template <class Cat, int L, int LP, bool INV, int B, int NT, int NS, int R0, int... Rs>
+template <class Cat, int L, int LP, bool INV, int B, int NT, bool OPQ, int NS, int R0, int... Rs>
 __device__ __forceinline__ void fft_stages(float2 *s, const float2 *tw)
 {
-    fft_stage<Cat, L, LP, R0, NS, INV, B, NT>(s, tw);
-    if constexpr (sizeof...(Rs) > 0) fft_stages<Cat, L, LP, INV, B, NT, NS * R0, Rs...>(s, tw);
+    fft_stage<Cat, L, LP, R0, NS, INV, B, NT, OPQ>(s, tw);
+    if constexpr (sizeof...(Rs) > 0) fft_stages<Cat, L, LP, INV, B, NT, OPQ, NS * R0, Rs...>(s, tw);
 }
 
-template <class Cat, int L, int LP, bool INV, int B, int NT, int... Rs>
+template <class Cat, int L, int LP, bool INV, int B, int NT, bool OPQ = false, int... Rs>
 __device__ __forceinline__ void fft_run(float2 *s, const float2 *tw, Radices<Rs...>)
 {
     static_assert((1 * ... * Rs) == L, "radix plan does not multiply to L");
-    fft_stages<Cat, L, LP, INV, B, NT, 1, Rs...>(s, tw);
+    fft_stages<Cat, L, LP, INV, B, NT, OPQ, 1, Rs...>(s, tw);
 }
 
 }  // namespace dns2d

@@ -25,6 +25,8 @@ struct KernelSet {
     void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, cudaStream_t);
     // full 2D R2C of the physical u, w planes (dump path; nullptr at the cluster sizes)
     void (*velocity_r2c_full)(const Pointers &, const float *, float2 *, cudaStream_t);
+    // min / max partials rows_scalar leaves in its `mm` argument (0: none that cover its output)
+    int scalar_parts;
 };
 
 template <int N>
@@ -161,7 +163,7 @@ struct Launch {
                          cols_step, cols_init,
                          rows_velocity,
                          rows_from_phys, cols_scalar, rows_scalar, rows_fwd_scalar, cols_fwd_scalar,
-                         velocity_r2c_full};
+                         velocity_r2c_full, V2 ? C::L / 2 : GB};
     }
 };
 
@@ -218,7 +220,7 @@ struct LaunchC {
     static KernelSet make()
     {
         return KernelSet{N, 1, 4 * C::L, &TwCatC<N>::cat, setup, rows_step, cols_step, cols_init, rows_velocity,
-                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr, nullptr};
+                         rows_from_phys, cols_scalar, rows_scalar, nullptr, nullptr, nullptr, 0};
     }
 };
 

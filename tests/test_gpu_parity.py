@@ -135,7 +135,10 @@ def test_omega_phys_and_sigma_match_oracle(N):
     w_gpu = s.phys(2).astype(np.float64)
     w_ref = o.omega_phys()
     assert rel_l2(w_gpu, w_ref) < 2e-6
-    assert int(s.display_sigma(2)) == int(O.display_sigma(w_ref))
+    sig = s.display_sigma(2)  # from OM2PHYS's own min / max partials
+    assert int(sig) == int(O.display_sigma(w_ref))
+    s.display_sigma(0)  # a min / max pass of another plane replaces those partials
+    assert s.display_sigma(2) == sig  # plane 2 by its own min / max pass: the same value
     # stream function: psi = inverse transform of om2 / K^2 (0 at k = 0)
     s.stream_func()
     psi = s.phys(2).astype(np.float64)
