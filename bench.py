@@ -527,15 +527,15 @@ def main_reference(args, runs: int = 3):
     print(json.dumps(line), flush=True)
 
 
-def main_ensemble(args):
-    """64 independent decaying runs (32 x N=128, 24 x N=256, 8 x N=512; Re log-uniform in
-    [1e3, 1e5], K0 in [2, 8], seeds 0..63, CFL 0.1) advanced together; NEXTDT every UPDATE steps."""
+def time_ensemble(ms, K, W, up, mode, tune, clocks=None):
+    """Device time (ms) of K ensemble steps after W warm-up steps, NEXTDT every UPDATE steps:
+    mode 0 = one graph per chunk (a branch per size group), 1 = one persistent launch per chunk."""
     import torch
     import optimizec_b200 as P
-    ms = P.ensemble_members()
-    K, W, up = args.steps, args.warmup, WORKLOAD["UPDATE"]
     b = P.Batch(ms)
-    b.autotune()  # each size group's kernel variants at its own member count
+    if tune:
+        b.autotune()  # each size group's kernel variants at its own member count
+    b.set_mode(mode)
     b.init_k4()
     b.next_dt()
     it = 0
@@ -549,21 +549,35 @@ def main_ensemble(args):
             if it == 1 or it % up == 0:
                 b.next_dt()
     advance(W)
-    for n in set(segments(W, W + K, up)):  # graph capture stays out of the timed region
-        b.prepare(n)
+    if mode == 0:
+        for n in set(segments(W, W + K, up)):  # graph capture stays out of the timed region
+            b.prepare(n)
     b.sync()
     stream = torch.cuda.ExternalStream(b.stream(), device=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(0)
-    clocks.start()
-    time.sleep(0.3)
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
     e0.record(stream)
     advance(W + K)
     e1.record(stream)
     b.sync()
     torch.cuda.synchronize()
-    ck = clocks.stop()
-    ms_ = e0.elapsed_time(e1)
+    ck = clocks.stop() if clocks else None
+    b.close()
+    return e0.elapsed_time(e1), ck
+
+
+def main_ensemble(args):
+    """64 independent decaying runs (32 x N=128, 24 x N=256, 8 x N=512; Re log-uniform in
+    [1e3, 1e5], K0 in [2, 8], seeds 0..63, CFL 0.1) advanced together; NEXTDT every UPDATE steps.
+    The line's value is the default stepping mode (one graph per chunk, autotuned); the persistent
+    launch (every member in one cooperative kernel per chunk) is timed beside it."""
+    import optimizec_b200 as P
+    ms = P.ensemble_members()
+    K, W, up = args.steps, args.warmup, WORKLOAD["UPDATE"]
+    ms_, ck = time_ensemble(ms, K, W, up, 0, True, ClockSampler(0))
+    ms_p, _ = time_ensemble(ms, K, W, up, 1, False)
     member_steps = len(ms) * K / (ms_ / 1e3)
     pts = sum(m[0] ** 2 for m in ms)
     peak, peak_kind = measured_peaks()
@@ -577,9 +591,12 @@ def main_ensemble(args):
                        "autotuned": "per size group at its member count (dns2d_batch_autotune)"},
             "ensemble_steps_per_s": round(K / (ms_ / 1e3), 2),
             "mpts_steps_per_s": round(pts * K / (ms_ / 1e3) / 1e6, 1),
-            "hbm_frac_64N2": round(byts * K / (ms_ / 1e3) / (peak * 1e9), 4), "clocks": ck}
+            "hbm_frac_64N2": round(byts * K / (ms_ / 1e3) / (peak * 1e9), 4), "clocks": ck,
+            "persistent_launch": {"ms_per_step": round(ms_p / K, 5),
+                                  "member_steps_s": round(len(ms) * K / (ms_p / 1e3), 1),
+                                  "what": "dns2d_batch_set_mode(1): every member in one cooperative kernel per "
+                                          "chunk, default radix plans, 8 row tiles / 4 column groups per item"}}
     print(json.dumps(line), flush=True)
-    b.close()
 
 
 def main_profile(args):

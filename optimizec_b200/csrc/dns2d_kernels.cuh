@@ -792,6 +792,24 @@ __device__ __forceinline__ void stage1g_last_band(float2 *s, const float2 *tw, i
     }
 }
 
+// Where one column CTA holds an SM (MC4 = 1), the column's om2 / fnm1 are brought into shared
+// memory by cp.async at the start of the column pass, behind the D, E columns, so the spectral
+// update reads them with no global-load latency left (N = 4096 on B200: column pass 0.299 ->
+// 0.294 ms).  With two CTAs per SM the 2 x 16 N bytes more shrink L1 below the twiddle tables
+// (N = 2048: 0.075 -> 0.076 ms), so there the state is read from global memory, prefetched to L2.
+template <int N>
+constexpr bool cols4_stage_state()
+{
+    return Cfg2<N>::MC4 == 1;
+}
+
+// dynamic shared memory of k_cols_step4: the D / E (then U / W) arrays and the staged state
+template <int N>
+constexpr size_t cols4_smem_bytes()
+{
+    return (2 * (size_t)Cfg2<N>::LP + (cols4_stage_state<N>() ? 2 * (size_t)N : 0)) * sizeof(float2);
+}
+
 template <int N>
 __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Pointers p0, int first, int hist_slot)
 {
@@ -813,9 +831,19 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
     float2 *fnc = p.fnm1 + (size_t)kx * N;
     for (int z = j; z < L; z += NT) cp_async8(sg + sidx<PS>(z), p.work + widx<L, H>(g, z, kx));
     cp_async_commit();
-    for (int o = (int)threadIdx.x * 16; o < N; o += NT2 * 16) {
-        prefetch_l2(om2c + o);
-        prefetch_l2(fnc + o);
+    constexpr bool STAGE = cols4_stage_state<N>();
+    float2 *so = smem + 2 * LP, *sf = so + N;  // the staged state column, dense (read at consecutive iz)
+    if constexpr (STAGE) {
+        for (int i = (int)threadIdx.x; i < N; i += NT2) {
+            cp_async8(so + i, om2c + i);
+            cp_async8(sf + i, fnc + i);
+        }
+        cp_async_commit();
+    } else {
+        for (int o = (int)threadIdx.x * 16; o < N; o += NT2 * 16) {
+            prefetch_l2(om2c + o);
+            prefetch_l2(fnc + o);
+        }
     }
     if (p.pf_cols > 0 && kx + p.pf_cols < (int)gridDim.x) {  // the column pf_cols CTAs later
         const int kp = kx + p.pf_cols;
@@ -824,11 +852,12 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
             prefetch_l2(p.work + (size_t)a * L * H + (((size_t)gg * H + kp) << 2));
         }
     }
-    cp_async_wait<0>();
+    cp_async_wait<STAGE ? 1 : 0>();  // this thread's D / E copies have landed
     stage1g<TwCat<N>, L, R3, 1, false, NT, PS>(sg, p.tw, j, bar);
     stage1g<TwCat<N>, L, R2, R3, false, NT, PS>(sg, p.tw, j, bar);
     // the update reads kz_i < H and kz_i >= L - H only: the 3/2 band [H, L-H-1] is not stored
     stage1g_last_band<TwCat<N>, L, R1, false, NT, H, L - H - 1, PS>(sg, p.tw, j, bar);
+    cp_async_wait<0>();  // and the state copies
     __syncthreads();
 
     const StepParams prm = *p.prm;
@@ -854,7 +883,8 @@ __global__ void __launch_bounds__(2 * Cfg2<N>::NT, Cfg2<N>::MC4) k_cols_step4(Po
             if (p.force) fn = add_forcing(fn, p, kx, iz, N);
         }
         const double K2 = (double)kx * kx + (double)kz * kz;
-        const float2 on = cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
+        const float2 on = STAGE ? cn_update(so[iz], fn, sf[iz], K2, hvdt, c2n, c3n)
+                                : cn_update(om2c[iz], fn, fnc[iz], K2, hvdt, c2n, c3n);
         om2c[iz] = on;
         fnc[iz] = fn;
         float2 u, w;

@@ -74,7 +74,7 @@ struct Launch {
         if constexpr (V2) {
             if ((e = cudaFuncSetAttribute(k_rows_step2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_step2<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
-            if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)(2 * sm2))) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k_cols_step4<N>, a, (int)cols4_smem_bytes<N>())) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_rows_velocity2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_cols_scalar2<N>, a, (int)sm2)) != cudaSuccess) return e;
             if ((e = cudaFuncSetAttribute(k_rows_pair2<N>, a, (int)sm2)) != cudaSuccess) return e;
@@ -112,7 +112,7 @@ struct Launch {
         // B200 at N = 1024, 2048 and 4096); both give the same arithmetic
         if constexpr (V2) {
             const int g = p.cols_groups ? p.cols_groups : 2;
-            if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
+            if (g == 2) k_cols_step4<N><<<dim3(C::H, ny), 2 * Cfg2<N>::NT, cols4_smem_bytes<N>(), s>>>(p, first, slot);
             else k_cols_step2<N><<<dim3(C::H, ny), Cfg2<N>::NT, 2 * sm2, s>>>(p, first, slot);
         }
         else if (p.plan_cols == 1) k_cols_step<N, P1><<<dim3(C::H, ny), C::NTA, smA, s>>>(p, first, slot);
