@@ -446,13 +446,13 @@ struct Cfg2 {
         static_assert(R1_ * R2_ * R3_ == L, "plan");                                           \
         static_assert(L / R1_ <= NT_ && L / R2_ <= NT_ && L / R3_ <= NT_, "one butterfly");    \
     };
-// N = 4096: plan (16, 24, 16) with padding every 16 elements makes every shared-memory access of
-// both passes bank-conflict free (the radix-24 stage has Ns = 16, so its stores are contiguous per
+// N = 4096 / 2048: plans (16, 24, 16) / (16, 12, 16) with padding every 16 elements make every
+// shared-memory access of both passes bank-conflict free (the radix-24 stage has Ns = 16, so its stores are contiguous per
 // half-warp, and the stride-16 stores of the Ns = 1 stages spread over all banks); the radix-16
 // middle stage of the row pass also holds 16 values in registers instead of 24.
 //          N    NT  plan (R1, R2, R3)  column CTAs per SM asked of the register allocator, pad
-DNS2D_CFG2(1024, 192, 16, 8, 12,       2, 1, 5)
-DNS2D_CFG2(2048, 256, 16, 16, 12,      2, 2, 5)  // two-group columns at 64 registers, 2 CTAs per SM
+DNS2D_CFG2(1024, 192, 16, 12, 8,       2, 1, 4)
+DNS2D_CFG2(2048, 256, 16, 12, 16,      2, 2, 4)  // two-group columns at 64 registers, 2 CTAs per SM
 DNS2D_CFG2(4096, 384, 16, 24, 16,      2, 1, 4)
 #undef DNS2D_CFG2
 

@@ -121,3 +121,24 @@ def test_window_plan():
     assert bench.window_plan(5, 20, 100, 0.6) == [5 + 20 * i for i in range(84)]
     assert bench.window_plan(100, 500, 100, 0.6) == [100, 600, 1100, 1600]
     assert len(bench.window_plan(5, 20, 100, 1e-9)) == 200
+
+
+def test_reference_arm_initial_field(tmp_path):
+    """The reference arm's restart.bin: the workload's seeded k^4 field at step 0 with the FP64
+    oracle's NEXTDT-init dt, in the v2 layout the reference's loader reads (a small N here)."""
+    import struct
+    import numpy as np
+    import bench
+    from oracle import oracle as O
+    bench.select_workload("dns4096", 32)
+    try:
+        path = str(tmp_path / "restart.bin")
+        note = bench.reference_initial_field(32, path)
+        assert "k^4" in note
+        b = open(path, "rb").read()
+        h = struct.unpack("<16s4I10i9f4x4Q", b[:144])
+        assert h[5] == 32 and h[13] == 0 and h[19] > 0  # N, it, dt
+        om = np.frombuffer(b, dtype=np.complex64, count=32 * 16, offset=144 + 3 * 48 * 48 * 4).reshape(32, 16)
+        assert np.array_equal(om, O.k4_spectrum(32, 4.0, 0))
+    finally:
+        bench.select_workload("dns4096", None)
