@@ -37,29 +37,35 @@ struct Cfg;
 template <int N>
 struct TwCat;
 
-#define DNS2D_CFG(N_, ROWS_, NTB_, NTA_, ...)                                                  \
+#define DNS2D_CFG(N_, ROWS_, NTB_, NTA_, PS_, EX_, ...)                                      \
     template <>                                                                                \
     struct Cfg<N_> {                                                                           \
         static constexpr int N = N_;                                                           \
         static constexpr int H = N_ / 2;                                                       \
         static constexpr int L = 3 * N_ / 2;                                                   \
-        static constexpr int LP = SmemLen<L>::value;                                           \
+        static constexpr int PS = PS_; /* shared-memory padding: one float2 every 2^PS */      \
+        static constexpr int LP = SmemLen<L, PS_, EX_>::value;                                 \
         static constexpr int ROWS = ROWS_;                                                     \
         static constexpr int NTB = NTB_;                                                       \
         static constexpr int NTA = NTA_;                                                       \
         using Plan = Radices<__VA_ARGS__>;                                                     \
     };
 
-//          N     ROWS  NTB  NTA  radix plan (product = 3N/2)
-DNS2D_CFG(16,    4,   64,  32,  4, 6)
-DNS2D_CFG(32,    4,   64,  32,  8, 6)
-DNS2D_CFG(64,    4,  128,  64,  8, 12)
-DNS2D_CFG(128,   4,  192,  64,  16, 12)
-DNS2D_CFG(256,   4,  256, 128,  16, 24)
-DNS2D_CFG(512,   4,  384, 192,  16, 16, 3)
-DNS2D_CFG(1024,  4,  512, 256,  16, 8, 12)
-DNS2D_CFG(2048,  4,  768, 384,  16, 16, 12)
-DNS2D_CFG(4096,  2,  768, 768,  16, 16, 24)
+// Padding (PS) and array stride (EX, the float2 added to the 16-rounded padded length) of the
+// small sizes, chosen with a model of the half-warp bank conflicts of every stage of their three
+// radix plans, rows (4 or 8 arrays per CTA) and columns (2 arrays); e.g. N = 128, plan (16, 12):
+// 2.0x / 1.71x the conflict-free wavefronts with one float2 every 32 and arrays 4 apart, 1.12x /
+// 1.07x with one every 16 and arrays 12 apart; N = 512, plan (16, 16, 3): 1.17x -> 1.0x.
+//          N     ROWS  NTB  NTA  PS EX  radix plan (product = 3N/2)
+DNS2D_CFG(16,    4,   64,  32,  5, 4,  4, 6)
+DNS2D_CFG(32,    4,   64,  32,  5, 4,  8, 6)
+DNS2D_CFG(64,    4,  128,  64,  4, 8,  8, 12)
+DNS2D_CFG(128,   4,  192,  64,  4, 12, 16, 12)
+DNS2D_CFG(256,   4,  256, 128,  4, 9,  16, 24)
+DNS2D_CFG(512,   4,  384, 192,  4, 0,  16, 16, 3)
+DNS2D_CFG(1024,  4,  512, 256,  5, 4,  16, 8, 12)
+DNS2D_CFG(2048,  4,  768, 384,  5, 4,  16, 16, 12)
+DNS2D_CFG(4096,  2,  768, 768,  5, 4,  16, 16, 24)
 #undef DNS2D_CFG
 
 // Alternative radix plans of the small-grid row and column passes (k_rows_step, k_cols_step),
@@ -227,7 +233,7 @@ __device__ __forceinline__ double2 block_sum2(double2 v, double2 *red)
 
 // Hermitian packing of two real rows' half spectra a = F[u], b = F[w] (kx < H) into the full
 // complex spectrum of u + i w.  Like a C2R transform, only Re of the kx = 0 entries is used.
-template <int L, int H, int ROWS, int NT, int LP>
+template <int L, int H, int ROWS, int NT, int LP, int PS = 5>
 __device__ __forceinline__ void rows_load_pack(float2 *s, const float2 *__restrict__ work, int z0)
 {
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
@@ -236,16 +242,16 @@ __device__ __forceinline__ void rows_load_pack(float2 *s, const float2 *__restri
         const float2 b = work[widx<L, H>(1, z0 + r, k)];
         float2 *x = s + r * LP;
         if (k == 0) {
-            x[sidx(0)] = make_float2(a.x, b.x);
+            x[sidx<PS>(0)] = make_float2(a.x, b.x);
         } else {
-            x[sidx(k)] = make_float2(a.x - b.y, a.y + b.x);
-            x[sidx(L - k)] = make_float2(a.x + b.y, b.x - a.y);
+            x[sidx<PS>(k)] = make_float2(a.x - b.y, a.y + b.x);
+            x[sidx<PS>(L - k)] = make_float2(a.x + b.y, b.x - a.y);
         }
     }
     constexpr int NZ = L - 2 * H + 1;  // zero band kx in [H, L-H]
     for (int e = threadIdx.x; e < ROWS * NZ; e += NT) {
         const int r = e / NZ, k = H + (e - r * NZ);
-        s[r * LP + sidx(k)] = make_float2(0.f, 0.f);
+        s[r * LP + sidx<PS>(k)] = make_float2(0.f, 0.f);
     }
 }
 
@@ -257,27 +263,28 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_step(Pointers p0)
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTB;
     extern __shared__ float2 smem[];
     const int z0 = blockIdx.x * ROWS;
-    rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
+    rows_load_pack<L, H, ROWS, NT, LP, PS>(smem, p.work, z0);
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT, PS>(smem, p.tw, Plan{});
     // products: (u + i w)^2 = (u^2 - w^2) + i (2 u w)
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
-        float2 *a = smem + r * LP + sidx(x);
+        float2 *a = smem + r * LP + sidx<PS>(x);
         const float2 z = *a;
         *a = make_float2(z.x * z.x - z.y * z.y, 2.0f * z.x * z.y);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT, PS>(smem, p.tw, Plan{});
     // unpack: D = F[u^2 - w^2] = (Q[k] + conj Q[L-k]) / 2, E = F[u w] = -i (Q[k] - conj Q[L-k]) / 4
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
         const float2 *x = smem + r * LP;
-        const float2 q = x[sidx(k)];
-        const float2 m = x[sidx(k == 0 ? 0 : L - k)];
+        const float2 q = x[sidx<PS>(k)];
+        const float2 m = x[sidx<PS>(k == 0 ? 0 : L - k)];
         p.work[widx<L, H>(0, z0 + r, k)] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
         p.work[widx<L, H>(1, z0 + r, k)] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
     }
@@ -336,6 +343,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
     __shared__ double2 red[32];
@@ -343,11 +351,11 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
     const int kx = blockIdx.x;
     float2 *sD = smem, *sE = smem + LP;
     for (int z = threadIdx.x; z < L; z += NT) {
-        sD[sidx(z)] = p.work[widx<L, H>(0, z, kx)];
-        sE[sidx(z)] = p.work[widx<L, H>(1, z, kx)];
+        sD[sidx<PS>(z)] = p.work[widx<L, H>(0, z, kx)];
+        sE[sidx<PS>(z)] = p.work[widx<L, H>(1, z, kx)];
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, 2, NT>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, false, 2, NT, PS>(smem, p.tw, Plan{});
 
     const StepParams prm = *p.prm;
     const float dt = prm.dt;
@@ -364,8 +372,8 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
     for (int iz = threadIdx.x; iz < N; iz += NT) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
-        const float2 d = sD[sidx(kzi)];
-        const float2 e = sE[sidx(kzi)];
+        const float2 d = sD[sidx<PS>(kzi)];
+        const float2 e = sE[sidx<PS>(kzi)];
         float2 fn = make_float2(0.f, 0.f);
         if (kz != -H) {  // STEP2B zeroes the kz = -N/2 row (cuda/step2b_cuda.cu:203-221)
             const float ga = (float)kz * (float)kx;
@@ -381,15 +389,15 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
         float2 u, w;
         double invK2;
         recover_velocity(kx, kz, on, u, w, invK2);
-        sD[sidx(kzi)] = u;
-        sE[sidx(kzi)] = w;
+        sD[sidx<PS>(kzi)] = u;
+        sE[sidx<PS>(kzi)] = w;
         const double pw = (double)on.x * on.x + (double)on.y * on.y;
         ez.x += wgt * pw * invK2;
         ez.y += wgt * pw;
     }
     for (int z = H + threadIdx.x; z < L - H; z += NT) {  // 3/2 zero padding in kz
-        sD[sidx(z)] = make_float2(0.f, 0.f);
-        sE[sidx(z)] = make_float2(0.f, 0.f);
+        sD[sidx<PS>(z)] = make_float2(0.f, 0.f);
+        sE[sidx<PS>(z)] = make_float2(0.f, 0.f);
     }
     // energy / enstrophy of the updated field: per-column partials, the last block sums them
     // in column order (deterministic)
@@ -415,10 +423,10 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_step(Pointers p0, int firs
         }
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, 2, NT>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, true, 2, NT, PS>(smem, p.tw, Plan{});
     for (int z = threadIdx.x; z < L; z += NT) {
-        p.work[widx<L, H>(0, z, kx)] = sD[sidx(z)];
-        p.work[widx<L, H>(1, z, kx)] = sE[sidx(z)];
+        p.work[widx<L, H>(0, z, kx)] = sD[sidx<PS>(z)];
+        p.work[widx<L, H>(1, z, kx)] = sE[sidx<PS>(z)];
     }
 }
 
@@ -1059,6 +1067,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p0, const fl
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
     const int kx = blockIdx.x;
@@ -1079,18 +1088,18 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_init(Pointers p0, const fl
             double invK2;
             recover_velocity(kx, kz, p.om2[(size_t)kx * N + iz], u, w, invK2);
         }
-        sU[sidx(kzi)] = u;
-        sW[sidx(kzi)] = w;
+        sU[sidx<PS>(kzi)] = u;
+        sW[sidx<PS>(kzi)] = w;
     }
     for (int z = H + threadIdx.x; z < L - H; z += NT) {
-        sU[sidx(z)] = make_float2(0.f, 0.f);
-        sW[sidx(z)] = make_float2(0.f, 0.f);
+        sU[sidx<PS>(z)] = make_float2(0.f, 0.f);
+        sW[sidx<PS>(z)] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, 2, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, 2, NT, PS>(smem, p.tw, typename C::Plan{});
     for (int z = threadIdx.x; z < L; z += NT) {
-        p.work[widx<L, H>(0, z, kx)] = sU[sidx(z)];
-        p.work[widx<L, H>(1, z, kx)] = sW[sidx(z)];
+        p.work[widx<L, H>(0, z, kx)] = sU[sidx<PS>(z)];
+        p.work[widx<L, H>(1, z, kx)] = sW[sidx<PS>(z)];
     }
 }
 
@@ -1104,17 +1113,18 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_velocity(Pointers p0, floa
 {
     const Pointers p = p0.member(blockIdx.y);
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
     __shared__ float red[32];
     const int z0 = blockIdx.x * ROWS;
-    rows_load_pack<L, H, ROWS, NT, LP>(smem, p.work, z0);
+    rows_load_pack<L, H, ROWS, NT, LP, PS>(smem, p.work, z0);
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT, PS>(smem, p.tw, typename C::Plan{});
     float m = 0.0f;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
-        const float2 z = smem[r * LP + sidx(x)];
+        const float2 z = smem[r * LP + sidx<PS>(x)];
         if (phys) {
             const size_t o = (size_t)(z0 + r) * L + x;
             phys[o] = z.x;
@@ -1135,22 +1145,23 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_from_phys(Pointers p, const float *phys)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
     const int z0 = blockIdx.x * ROWS;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
         const size_t o = (size_t)(z0 + r) * L + x;
-        smem[r * LP + sidx(x)] = make_float2(phys[o], phys[(size_t)L * L + o]);
+        smem[r * LP + sidx<PS>(x)] = make_float2(phys[o], phys[(size_t)L * L + o]);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT, PS>(smem, p.tw, typename C::Plan{});
     const float sc = 1.0f / (float)L;
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
         const float2 *x = smem + r * LP;
-        const float2 q = x[sidx(k)];
-        const float2 m = x[sidx(k == 0 ? 0 : L - k)];
+        const float2 q = x[sidx<PS>(k)];
+        const float2 m = x[sidx<PS>(k == 0 ? 0 : L - k)];
         p.work[widx<L, H>(0, z0 + r, k)] = make_float2(0.5f * sc * (q.x + m.x), 0.5f * sc * (q.y - m.y));
         p.work[widx<L, H>(1, z0 + r, k)] = make_float2(0.5f * sc * (q.y + m.y), -0.5f * sc * (q.x - m.x));
     }
@@ -1165,6 +1176,7 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_scalar(Pointers p, float2 *scratch, int kind)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
     const int kx = blockIdx.x;
@@ -1177,12 +1189,12 @@ __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_scalar(Pointers p, float2 
             v = make_float2(v.x / k2, v.y / k2);
             if (kx == 0 && iz == 0) v = make_float2(0.f, 0.f);
         }
-        smem[sidx(kzi)] = v;
+        smem[sidx<PS>(kzi)] = v;
     }
-    for (int z = H + threadIdx.x; z < L - H; z += NT) smem[sidx(z)] = make_float2(0.f, 0.f);
+    for (int z = H + threadIdx.x; z < L - H; z += NT) smem[sidx<PS>(z)] = make_float2(0.f, 0.f);
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, 1, NT>(smem, p.tw, typename C::Plan{});
-    for (int z = threadIdx.x; z < L; z += NT) scratch[widx<L, H>(0, z, kx)] = smem[sidx(z)];
+    fft_run<TwCat<N>, L, LP, true, 1, NT, PS>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) scratch[widx<L, H>(0, z, kx)] = smem[sidx<PS>(z)];
 }
 
 // scratch rows -> real field rows written to out ([L][L]); per-block min/max partials
@@ -1191,6 +1203,7 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_scalar(Pointers p, const f
                                                              float2 *minmax)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
     __shared__ float red[32];
@@ -1200,23 +1213,23 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_scalar(Pointers p, const f
         const float2 a = scratch[widx<L, H>(0, z0 + r, k)];
         float2 *x = smem + r * LP;
         if (k == 0) {
-            x[sidx(0)] = make_float2(a.x, 0.f);
+            x[sidx<PS>(0)] = make_float2(a.x, 0.f);
         } else {
-            x[sidx(k)] = a;
-            x[sidx(L - k)] = make_float2(a.x, -a.y);
+            x[sidx<PS>(k)] = a;
+            x[sidx<PS>(L - k)] = make_float2(a.x, -a.y);
         }
     }
     constexpr int NZ = L - 2 * H + 1;
     for (int e = threadIdx.x; e < ROWS * NZ; e += NT) {
         const int r = e / NZ, k = H + (e - r * NZ);
-        smem[r * LP + sidx(k)] = make_float2(0.f, 0.f);
+        smem[r * LP + sidx<PS>(k)] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT, PS>(smem, p.tw, typename C::Plan{});
     float mn = 3.402823466e38f, mx = -3.402823466e38f;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
-        const float v = smem[r * LP + sidx(x)].x;
+        const float v = smem[r * LP + sidx<PS>(x)].x;
         out[(size_t)(z0 + r) * L + x] = v;
         mn = fminf(mn, v);
         mx = fmaxf(mx, v);
@@ -1238,19 +1251,20 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_fwd_scalar(Pointers p, const float *f, float2 *scratch)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = C::ROWS, NT = C::NTB;
     extern __shared__ float2 smem[];
     const int z0 = blockIdx.x * ROWS;
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
-        smem[r * LP + sidx(x)] = make_float2(f[(size_t)(z0 + r) * L + x], 0.f);
+        smem[r * LP + sidx<PS>(x)] = make_float2(f[(size_t)(z0 + r) * L + x], 0.f);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT, PS>(smem, p.tw, typename C::Plan{});
     const float sc = 1.0f / (float)L;
     for (int e = threadIdx.x; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
-        const float2 q = smem[r * LP + sidx(k)];
+        const float2 q = smem[r * LP + sidx<PS>(k)];
         scratch[widx<L, H>(0, z0 + r, k)] = make_float2(q.x * sc, q.y * sc);
     }
 }
@@ -1259,17 +1273,18 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_fwd_scalar(Pointers p, const float2 *scratch, float2 *out)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
     const int kx = blockIdx.x;
-    for (int z = threadIdx.x; z < L; z += NT) smem[sidx(z)] = scratch[widx<L, H>(0, z, kx)];
+    for (int z = threadIdx.x; z < L; z += NT) smem[sidx<PS>(z)] = scratch[widx<L, H>(0, z, kx)];
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, 1, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, 1, NT, PS>(smem, p.tw, typename C::Plan{});
     const float sc = 1.0f / (float)L;
     for (int iz = threadIdx.x; iz < N; iz += NT) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
-        const float2 v = smem[sidx(kzi)];
+        const float2 v = smem[sidx<PS>(kzi)];
         out[(size_t)kx * N + iz] = (kz == -H) ? make_float2(0.f, 0.f) : make_float2(v.x * sc, v.y * sc);
     }
 }
@@ -1285,6 +1300,7 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_r2c_full(Pointers p, const float *phys, float2 *spec)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, LP = C::LP, ROWS = C::ROWS, NT = C::NTB, NK = L / 2 + 1;
     extern __shared__ float2 smem[];
     const int z0 = blockIdx.x * ROWS;
@@ -1292,14 +1308,14 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_r2c_full(Pointers p, const
     for (int e = threadIdx.x; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
         const size_t i = (size_t)(z0 + r) * L + x;
-        smem[r * LP + sidx(x)] = make_float2(u[i], w[i]);
+        smem[r * LP + sidx<PS>(x)] = make_float2(u[i], w[i]);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, ROWS, NT>(smem, p.tw, typename C::Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT, PS>(smem, p.tw, typename C::Plan{});
     for (int e = threadIdx.x; e < ROWS * NK; e += NT) {
         const int r = e / NK, k = e - r * NK;
-        const float2 q = smem[r * LP + sidx(k)];
-        const float2 m = smem[r * LP + sidx(k == 0 ? 0 : L - k)];
+        const float2 q = smem[r * LP + sidx<PS>(k)];
+        const float2 m = smem[r * LP + sidx<PS>(k == 0 ? 0 : L - k)];
         const size_t o = (size_t)(z0 + r) * NK + k;
         spec[o] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
         spec[(size_t)L * NK + o] = make_float2(0.5f * (q.y + m.y), -0.5f * (q.x - m.x));
@@ -1310,13 +1326,14 @@ template <int N>
 __global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_c2c_full(Pointers p, float2 *spec)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     constexpr int L = C::L, LP = C::LP, NT = C::NTA, NK = L / 2 + 1;
     extern __shared__ float2 smem[];
     float2 *col = spec + (size_t)blockIdx.y * L * NK + blockIdx.x;
-    for (int z = threadIdx.x; z < L; z += NT) smem[sidx(z)] = col[(size_t)z * NK];
+    for (int z = threadIdx.x; z < L; z += NT) smem[sidx<PS>(z)] = col[(size_t)z * NK];
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, 1, NT>(smem, p.tw, typename C::Plan{});
-    for (int z = threadIdx.x; z < L; z += NT) col[(size_t)z * NK] = smem[sidx(z)];
+    fft_run<TwCat<N>, L, LP, false, 1, NT, PS>(smem, p.tw, typename C::Plan{});
+    for (int z = threadIdx.x; z < L; z += NT) col[(size_t)z * NK] = smem[sidx<PS>(z)];
 }
 
 }  // namespace dns2d

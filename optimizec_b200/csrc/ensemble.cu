@@ -35,6 +35,7 @@ template <int N, class Plan>
 __device__ __forceinline__ void ens_rows(const Pointers &p, int z0, float2 *smem)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     const int tid = opaque_tid();  // nothing of it hoisted out of the work loop
     constexpr int L = C::L, H = C::H, LP = C::LP, ROWS = kEnsRows, NT = kEnsThreads;
     for (int e = tid; e < ROWS * H; e += NT) {
@@ -43,32 +44,32 @@ __device__ __forceinline__ void ens_rows(const Pointers &p, int z0, float2 *smem
         const float2 b = __ldcg(p.work + widx<L, H>(1, z0 + r, k));
         float2 *x = smem + r * LP;
         if (k == 0) {
-            x[sidx(0)] = make_float2(a.x, b.x);
+            x[sidx<PS>(0)] = make_float2(a.x, b.x);
         } else {
-            x[sidx(k)] = make_float2(a.x - b.y, a.y + b.x);
-            x[sidx(L - k)] = make_float2(a.x + b.y, b.x - a.y);
+            x[sidx<PS>(k)] = make_float2(a.x - b.y, a.y + b.x);
+            x[sidx<PS>(L - k)] = make_float2(a.x + b.y, b.x - a.y);
         }
     }
     constexpr int NZ = L - 2 * H + 1;  // zero band kx in [H, L-H]
     for (int e = tid; e < ROWS * NZ; e += NT) {
         const int r = e / NZ, k = H + (e - r * NZ);
-        smem[r * LP + sidx(k)] = make_float2(0.f, 0.f);
+        smem[r * LP + sidx<PS>(k)] = make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, ROWS, NT, true>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, true, ROWS, NT, PS, true>(smem, p.tw, Plan{});
     for (int e = tid; e < ROWS * L; e += NT) {
         const int r = e / L, x = e - r * L;
-        float2 *a = smem + r * LP + sidx(x);
+        float2 *a = smem + r * LP + sidx<PS>(x);
         const float2 z = *a;
         *a = make_float2(z.x * z.x - z.y * z.y, 2.0f * z.x * z.y);
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, ROWS, NT, true>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, false, ROWS, NT, PS, true>(smem, p.tw, Plan{});
     for (int e = tid; e < ROWS * H; e += NT) {
         const int r = e % ROWS, k = e / ROWS;
         const float2 *x = smem + r * LP;
-        const float2 q = x[sidx(k)];
-        const float2 m = x[sidx(k == 0 ? 0 : L - k)];
+        const float2 q = x[sidx<PS>(k)];
+        const float2 m = x[sidx<PS>(k == 0 ? 0 : L - k)];
         p.work[widx<L, H>(0, z0 + r, k)] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
         p.work[widx<L, H>(1, z0 + r, k)] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
     }
@@ -84,17 +85,18 @@ __device__ __forceinline__ void ens_cols(const Pointers &p, int item, int first,
                                          double2 *red, int *last)
 {
     using C = Cfg<N>;
+    constexpr int PS = C::PS;
     const int tid = opaque_tid();  // nothing of it hoisted out of the work loop
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = kEnsThreads, CG = ens_cols_per_item<N>(), B = 2 * CG;
     const int kx0 = item * CG;
     // (z, kx0 + c) for c < CG and z%4 are CG * 4 consecutive float2 of a 4-row tile: read them so
     for (int e = tid; e < CG * L; e += NT) {
         const int z4 = e / (CG * 4), rem = e - z4 * (CG * 4), c = rem >> 2, z = 4 * z4 + (rem & 3);
-        smem[(2 * c) * LP + sidx(z)] = __ldcg(p.work + widx<L, H>(0, z, kx0 + c));
-        smem[(2 * c + 1) * LP + sidx(z)] = __ldcg(p.work + widx<L, H>(1, z, kx0 + c));
+        smem[(2 * c) * LP + sidx<PS>(z)] = __ldcg(p.work + widx<L, H>(0, z, kx0 + c));
+        smem[(2 * c + 1) * LP + sidx<PS>(z)] = __ldcg(p.work + widx<L, H>(1, z, kx0 + c));
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, false, B, NT, true>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, false, B, NT, PS, true>(smem, p.tw, Plan{});
 
     const StepParams prm = *p.prm;
     const float dt = prm.dt;
@@ -109,8 +111,8 @@ __device__ __forceinline__ void ens_cols(const Pointers &p, int item, int first,
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
         float2 *sD = smem + (2 * c) * LP, *sE = smem + (2 * c + 1) * LP;
-        const float2 d = sD[sidx(kzi)];
-        const float2 ee = sE[sidx(kzi)];
+        const float2 d = sD[sidx<PS>(kzi)];
+        const float2 ee = sE[sidx<PS>(kzi)];
         float2 fn = make_float2(0.f, 0.f);
         if (kz != -H) {  // STEP2B zeroes the kz = -N/2 row (cuda/step2b_cuda.cu:203-221)
             const float ga = (float)kz * (float)kx;
@@ -127,8 +129,8 @@ __device__ __forceinline__ void ens_cols(const Pointers &p, int item, int first,
         float2 u, w;
         double invK2;
         recover_velocity(kx, kz, on, u, w, invK2);
-        sD[sidx(kzi)] = u;
-        sE[sidx(kzi)] = w;
+        sD[sidx<PS>(kzi)] = u;
+        sE[sidx<PS>(kzi)] = w;
         const double pw = (double)on.x * on.x + (double)on.y * on.y;
         const double wgt = (kx == 0) ? 0.5 : 1.0;  // 1/2 * (1 on kx = 0, else 2)
         ez.x += wgt * pw * invK2;
@@ -137,8 +139,8 @@ __device__ __forceinline__ void ens_cols(const Pointers &p, int item, int first,
     constexpr int NZ = L - 2 * H;  // 3/2 zero padding in kz
     for (int e = tid; e < CG * NZ; e += NT) {
         const int c = e / NZ, z = H + (e - c * NZ);
-        smem[(2 * c) * LP + sidx(z)] = make_float2(0.f, 0.f);
-        smem[(2 * c + 1) * LP + sidx(z)] = make_float2(0.f, 0.f);
+        smem[(2 * c) * LP + sidx<PS>(z)] = make_float2(0.f, 0.f);
+        smem[(2 * c + 1) * LP + sidx<PS>(z)] = make_float2(0.f, 0.f);
     }
     ez = block_sum2<NT>(ez, red);
     if (tid == 0) {
@@ -162,11 +164,11 @@ __device__ __forceinline__ void ens_cols(const Pointers &p, int item, int first,
         }
     }
     __syncthreads();
-    fft_run<TwCat<N>, L, LP, true, B, NT, true>(smem, p.tw, Plan{});
+    fft_run<TwCat<N>, L, LP, true, B, NT, PS, true>(smem, p.tw, Plan{});
     for (int e = tid; e < CG * L; e += NT) {
         const int z4 = e / (CG * 4), rem = e - z4 * (CG * 4), c = rem >> 2, z = 4 * z4 + (rem & 3);
-        p.work[widx<L, H>(0, z, kx0 + c)] = smem[(2 * c) * LP + sidx(z)];
-        p.work[widx<L, H>(1, z, kx0 + c)] = smem[(2 * c + 1) * LP + sidx(z)];
+        p.work[widx<L, H>(0, z, kx0 + c)] = smem[(2 * c) * LP + sidx<PS>(z)];
+        p.work[widx<L, H>(1, z, kx0 + c)] = smem[(2 * c + 1) * LP + sidx<PS>(z)];
     }
 }
 

@@ -256,10 +256,12 @@ struct DFT {
 template <int PS = 5>
 __device__ __forceinline__ int sidx(int i) { return i + (i >> PS); }
 
-template <int L, int PS = 5>
+// array stride of L padded elements, rounded up to 16 float2 plus EX (EX = 4 by default: consecutive
+// arrays 8 banks apart)
+template <int L, int PS = 5, int EX = 4>
 struct SmemLen {
     static constexpr int raw = L + (L >> PS) + 1;
-    static constexpr int value = ((raw + 15) / 16) * 16 + 4;
+    static constexpr int value = ((raw + 15) / 16) * 16 + EX;
 };
 
 template <int... Rs>
@@ -325,7 +327,7 @@ __device__ __forceinline__ int opaque_tid()
 
 // One Stockham stage over B arrays of length L (array b at s + b*LP); OPQ: read the thread
 // index with opaque_tid().
-template <class Cat, int L, int LP, int R, int NS, bool INV, int B, int NT, bool OPQ = false>
+template <class Cat, int L, int LP, int R, int NS, bool INV, int B, int NT, int PS = 5, bool OPQ = false>
 __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *__restrict__ tw)
 {
     const int tid = OPQ ? opaque_tid() : (int)threadIdx.x;
@@ -341,7 +343,7 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *
             const int j = t - b * LR;
             const float2 *x = s + b * LP;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[i][r] = x[sidx(j + r * LR)];
+            for (int r = 0; r < R; ++r) v[i][r] = x[sidx<PS>(j + r * LR)];
             if constexpr (NS > 1) {
                 constexpr int OFF = Cat::off(R, NS);
                 static_assert(OFF >= 0, "stage missing from the twiddle catalog");
@@ -367,7 +369,7 @@ __device__ __forceinline__ void fft_stage(float2 *__restrict__ s, const float2 *
             const int k = j % NS;
             const int base = (j / NS) * NS * R + k;
 #pragma unroll
-            for (int q = 0; q < R; ++q) y[sidx(base + q * NS)] = v[i][q];
+            for (int q = 0; q < R; ++q) y[sidx<PS>(base + q * NS)] = v[i][q];
         }
     }
     __syncthreads();
@@ -510,18 +512,19 @@ __device__ __forceinline__ void cp_async_wait()
 }
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-template <class Cat, int L, int LP, bool INV, int B, int NT, bool OPQ, int NS, int R0, int... Rs>
+template <class Cat, int L, int LP, bool INV, int B, int NT, int PS, bool OPQ, int NS, int R0, int... Rs>
 __device__ __forceinline__ void fft_stages(float2 *s, const float2 *tw)
 {
-    fft_stage<Cat, L, LP, R0, NS, INV, B, NT, OPQ>(s, tw);
-    if constexpr (sizeof...(Rs) > 0) fft_stages<Cat, L, LP, INV, B, NT, OPQ, NS * R0, Rs...>(s, tw);
+    fft_stage<Cat, L, LP, R0, NS, INV, B, NT, PS, OPQ>(s, tw);
+    if constexpr (sizeof...(Rs) > 0) fft_stages<Cat, L, LP, INV, B, NT, PS, OPQ, NS * R0, Rs...>(s, tw);
 }
 
-template <class Cat, int L, int LP, bool INV, int B, int NT, bool OPQ = false, int... Rs>
+// PS: the padding of sidx<PS>; OPQ: read the thread index with opaque_tid()
+template <class Cat, int L, int LP, bool INV, int B, int NT, int PS = 5, bool OPQ = false, int... Rs>
 __device__ __forceinline__ void fft_run(float2 *s, const float2 *tw, Radices<Rs...>)
 {
     static_assert((1 * ... * Rs) == L, "radix plan does not multiply to L");
-    fft_stages<Cat, L, LP, INV, B, NT, OPQ, 1, Rs...>(s, tw);
+    fft_stages<Cat, L, LP, INV, B, NT, PS, OPQ, 1, Rs...>(s, tw);
 }
 
 }  // namespace dns2d
