@@ -37,25 +37,29 @@ struct CfgC {
     static constexpr bool enabled = false;
 };
 
-#define DNS2D_CFGC(N_, NT_, MINBR_, MINBC_, ...)                                               \
+#define DNS2D_CFGC(N_, NT_, MINBR_, MINBC_, PS_, ...)                                          \
     template <>                                                                                \
     struct CfgC<N_> {                                                                          \
         static constexpr bool enabled = true;                                                  \
-        static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, M = L / 4;                    \
-        static constexpr int MP = SmemLen<M>::value, NT = NT_, MINB_R = MINBR_, MINB_C = MINBC_; \
+        static constexpr int N = N_, H = N_ / 2, L = 3 * N_ / 2, M = L / 4, PS = PS_;          \
+        static constexpr int MP = SmemLen<M, PS_>::value, NT = NT_, MINB_R = MINBR_, MINB_C = MINBC_; \
         static constexpr int MQ = (M + 3) / 4; /* butterflies of the cluster radix per CTA */ \
         using Plan = Radices<__VA_ARGS__>;                                                     \
         static_assert(L % 4 == 0 && radix_product(Plan{}) == M, "plan");                       \
     };
 // NT threads per CTA (at least M / R for every radix R of the plan); CTAs per SM asked of the
 // register allocator for the row kernels (MINB_R) and the column kernels (MINB_C, two arrays of
-// shared memory and more live values), each the faster of the candidates measured on B200
-//           N      NT  MINB_R MINB_C  local radix plan (product = 3N/8)
-DNS2D_CFGC(840,    63,  1, 1,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
-DNS2D_CFGC(8192,  256,  4, 3,  16, 16, 12)  // L = 12288 = 4 x 3072
-DNS2D_CFGC(9216,  288,  4, 3,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
-DNS2D_CFGC(16384, 384,  3, 2,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
-DNS2D_CFGC(29400, 525,  1, 1,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
+// shared memory and more live values), each the faster of the candidates measured on B200;
+// shared-memory padding PS (one float2 every 2^PS) from the half-warp bank-conflict model of the
+// local plan's stages: every 16 makes the power-of-two-rich plans conflict-free (1.17x -> 1.0x
+// the ideal wavefronts at M = 3072 and 6144, 1.21x -> 1.08x at 3456), every 256 suits the odd
+// radices of M = 11025 (1.55x -> 1.32x)
+//           N      NT  MINB_R MINB_C PS  local radix plan (product = 3N/8)
+DNS2D_CFGC(840,    63,  1, 1,  5,  7, 5, 9)     // L = 1260 = 4 x 315 (test size of the cluster path)
+DNS2D_CFGC(8192,  256,  4, 3,  4,  16, 16, 12)  // L = 12288 = 4 x 3072
+DNS2D_CFGC(9216,  288,  4, 3,  4,  16, 12, 18)  // L = 13824 = 4 x 3456 = 2^9 3^3
+DNS2D_CFGC(16384, 384,  3, 2,  4,  16, 16, 24)  // L = 24576 = 4 x 6144 (the reference's N=16384 runs)
+DNS2D_CFGC(29400, 525,  1, 1,  8,  21, 21, 25)  // L = 44100 = 4 x 11025 = 2^2 3^2 5^2 7^2
 #undef DNS2D_CFGC
 
 template <int N>
@@ -113,7 +117,7 @@ __device__ __forceinline__ void cross_fwd(float2 (&x)[4], const Peers &dst, int 
 #pragma unroll
     for (int r = 1; r < 4; ++r) x[r] = cmul(x[r], cross_tw<N>(tw, r, m));
 #pragma unroll
-    for (int r = 0; r < 4; ++r) dst.p[r][sidx(m)] = x[r];
+    for (int r = 0; r < 4; ++r) dst.p[r][sidx<CfgC<N>::PS>(m)] = x[r];
 }
 
 // inverse cluster butterfly for position m: P_c[m] from the 4 CTAs in, x[m + M s] out
@@ -121,7 +125,7 @@ template <int N>
 __device__ __forceinline__ void cross_inv(float2 (&x)[4], const Peers &src, int m, const float2 *tw)
 {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) x[r] = src.p[r][sidx(m)];
+    for (int r = 0; r < 4; ++r) x[r] = src.p[r][sidx<CfgC<N>::PS>(m)];
 #pragma unroll
     for (int r = 1; r < 4; ++r) x[r] = cmul(x[r], cconj(cross_tw<N>(tw, r, m)));
     DFT<4, true>::run(x);
@@ -163,7 +167,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     // of the cluster runs before shared memory is written across it.
     for (int k2 = threadIdx.x; k2 < M; k2 += NT) {
         const int k = 4 * k2 + c;
-        if (k >= H && k <= L - H) s[sidx(k2)] = make_float2(0.f, 0.f);
+        if (k >= H && k <= L - H) s[sidx<CfgC<N>::PS>(k2)] = make_float2(0.f, 0.f);
     }
     cluster_sync_relaxed();
     {
@@ -172,16 +176,16 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         for (int k = k0 + (int)threadIdx.x; k < k1; k += NT) {
             const float2 a = U[(size_t)k << 2], b = W[(size_t)k << 2];
             if (k == 0) {
-                pe.p[0][sidx(0)] = make_float2(a.x, b.x);
+                pe.p[0][sidx<CfgC<N>::PS>(0)] = make_float2(a.x, b.x);
             } else {
-                pe.p[k & 3][sidx(k >> 2)] = make_float2(a.x - b.y, a.y + b.x);
+                pe.p[k & 3][sidx<CfgC<N>::PS>(k >> 2)] = make_float2(a.x - b.y, a.y + b.x);
                 const int km = L - k;
-                pe.p[km & 3][sidx(km >> 2)] = make_float2(a.x + b.y, b.x - a.y);
+                pe.p[km & 3][sidx<CfgC<N>::PS>(km >> 2)] = make_float2(a.x + b.y, b.x - a.y);
             }
         }
     }
     cl.sync();
-    fft_run<Cat, M, MP, true, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     const int m1 = min(M, (c + 1) * MQ);
     for (int m = c * MQ + threadIdx.x; m < m1; m += NT) {
@@ -192,7 +196,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         cross_fwd<N>(x, pe, m, p.tw);
     }
     cl.sync();
-    fft_run<Cat, M, MP, false, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, false, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     // unpack D = (Q[k] + conj Q[L-k]) / 2, E = -i (Q[k] - conj Q[L-k]) / 4 for k < H; Q[k] sits in
     // CTA k % 4 at position k / 4.  Each CTA writes a contiguous quarter of the k range.
@@ -203,8 +207,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         const int k0 = c * HQ, k1 = min(H, k0 + HQ);
         for (int k = k0 + (int)threadIdx.x; k < k1; k += NT) {
             const int kp = (k == 0) ? 0 : L - k;
-            const float2 q = pe.p[k & 3][sidx(k >> 2)];
-            const float2 m = pe.p[kp & 3][sidx(kp >> 2)];
+            const float2 q = pe.p[k & 3][sidx<CfgC<N>::PS>(k >> 2)];
+            const float2 m = pe.p[kp & 3][sidx<CfgC<N>::PS>(kp >> 2)];
             Do[(size_t)k << 2] = make_float2(0.5f * (q.x + m.x), 0.5f * (q.y - m.y));
             Eo[(size_t)k << 2] = make_float2(0.25f * (q.y + m.y), -0.25f * (q.x - m.x));
         }
@@ -300,8 +304,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         cross_fwd<N>(e, pE, m, p.tw);
     }
     cl.sync();
-    fft_run<Cat, M, MP, false, 1, NT>(sD, p.tw, typename C::Plan{});
-    fft_run<Cat, M, MP, false, 1, NT>(sE, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, false, 1, NT, CfgC<N>::PS>(sD, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, false, 1, NT, CfgC<N>::PS>(sE, p.tw, typename C::Plan{});
 
     const StepParams prm = *p.prm;
     const float dt = prm.dt;
@@ -318,12 +322,12 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         int kz;
         const int iz = iz_of_kzi<N>(4 * k2 + c, kz);
         if (iz < 0) {
-            sD[sidx(k2)] = make_float2(0.f, 0.f);
-            sE[sidx(k2)] = make_float2(0.f, 0.f);
+            sD[sidx<CfgC<N>::PS>(k2)] = make_float2(0.f, 0.f);
+            sE[sidx<CfgC<N>::PS>(k2)] = make_float2(0.f, 0.f);
             continue;
         }
-        const float2 d = sD[sidx(k2)];
-        const float2 e = sE[sidx(k2)];
+        const float2 d = sD[sidx<CfgC<N>::PS>(k2)];
+        const float2 e = sE[sidx<CfgC<N>::PS>(k2)];
         float2 fn = make_float2(0.f, 0.f);
         if (kz != -H) {
             const float ga = (float)kz * (float)kx;
@@ -339,8 +343,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         float2 u, w;
         double invK2;
         recover_velocity(kx, kz, on, u, w, invK2);
-        sD[sidx(k2)] = u;
-        sE[sidx(k2)] = w;
+        sD[sidx<CfgC<N>::PS>(k2)] = u;
+        sE[sidx<CfgC<N>::PS>(k2)] = w;
         const double pw = (double)on.x * on.x + (double)on.y * on.y;
         ez.x += wgt * pw * invK2;
         ez.y += wgt * pw;
@@ -348,8 +352,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     ez = block_sum2<NT>(ez, red);
     if (threadIdx.x == 0) cpart = ez;
     __syncthreads();
-    fft_run<Cat, M, MP, true, 1, NT>(sD, p.tw, typename C::Plan{});
-    fft_run<Cat, M, MP, true, 1, NT>(sE, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(sD, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(sE, p.tw, typename C::Plan{});
     cl.sync();
     cluster_energy<NT>(cl, p, kx, gridDim.x >> 2, &cpart, red, &am_last, hist_slot);
     for (int m = m0 + threadIdx.x; m < m1; m += NT) {
@@ -400,12 +404,12 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
                 recover_velocity(kx, kz, p.om2[(size_t)kx * N + iz], u, w, invK2);
             }
         }
-        sU[sidx(k2)] = u;
-        sW[sidx(k2)] = w;
+        sU[sidx<CfgC<N>::PS>(k2)] = u;
+        sW[sidx<CfgC<N>::PS>(k2)] = w;
     }
     __syncthreads();
-    fft_run<Cat, M, MP, true, 1, NT>(sU, p.tw, typename C::Plan{});
-    fft_run<Cat, M, MP, true, 1, NT>(sW, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(sU, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(sW, p.tw, typename C::Plan{});
     cl.sync();
     for (int m = c * MQ + threadIdx.x; m < min(M, (c + 1) * MQ); m += NT) {
         float2 x[4];
@@ -439,9 +443,9 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     const Peers pe(cl, s);
     const float2 *__restrict__ U = p.work + widx<L, H>(0, z, 0);
     const float2 *__restrict__ W = p.work + widx<L, H>(1, z, 0);
-    for (int k2 = threadIdx.x; k2 < M; k2 += NT) s[sidx(k2)] = packed_uw<L, H>(U, W, 4 * k2 + c);
+    for (int k2 = threadIdx.x; k2 < M; k2 += NT) s[sidx<CfgC<N>::PS>(k2)] = packed_uw<L, H>(U, W, 4 * k2 + c);
     __syncthreads();
-    fft_run<Cat, M, MP, true, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     float mx = 0.0f;
     for (int m = c * MQ + threadIdx.x; m < min(M, (c + 1) * MQ); m += NT) {
@@ -490,7 +494,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
         cross_fwd<N>(x, pe, m, p.tw);
     }
     cl.sync();
-    fft_run<Cat, M, MP, false, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, false, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     const float sc = 1.0f / (float)L;
     float2 *__restrict__ Uo = p.work + widx<L, H>(0, z, 0);
@@ -498,8 +502,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
     for (int k2 = threadIdx.x; 4 * k2 + c < H; k2 += NT) {
         const int k = 4 * k2 + c;
         const int kp = (k == 0) ? 0 : L - k;
-        const float2 q = s[sidx(k2)];
-        const float2 m = pe.p[kp & 3][sidx(kp >> 2)];
+        const float2 q = s[sidx<CfgC<N>::PS>(k2)];
+        const float2 m = pe.p[kp & 3][sidx<CfgC<N>::PS>(kp >> 2)];
         Uo[(size_t)k << 2] = make_float2(0.5f * sc * (q.x + m.x), 0.5f * sc * (q.y - m.y));
         Wo[(size_t)k << 2] = make_float2(0.5f * sc * (q.y + m.y), -0.5f * sc * (q.x - m.x));
     }
@@ -533,10 +537,10 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
                 if (kx == 0 && iz == 0) v = make_float2(0.f, 0.f);
             }
         }
-        s[sidx(k2)] = v;
+        s[sidx<CfgC<N>::PS>(k2)] = v;
     }
     __syncthreads();
-    fft_run<Cat, M, MP, true, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     for (int m = c * MQ + threadIdx.x; m < min(M, (c + 1) * MQ); m += NT) {
         float2 x[4];
@@ -573,10 +577,10 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(CfgC<N>::NT, CfgC<N>
             const float2 a = A[(size_t)(L - k) << 2];
             v = make_float2(a.x, -a.y);
         }
-        s[sidx(k2)] = v;
+        s[sidx<CfgC<N>::PS>(k2)] = v;
     }
     __syncthreads();
-    fft_run<Cat, M, MP, true, 1, NT>(s, p.tw, typename C::Plan{});
+    fft_run<Cat, M, MP, true, 1, NT, CfgC<N>::PS>(s, p.tw, typename C::Plan{});
     cl.sync();
     float mn = 3.402823466e38f, mx = -3.402823466e38f;
     for (int m = c * MQ + threadIdx.x; m < min(M, (c + 1) * MQ); m += NT) {
