@@ -3099,8 +3099,8 @@ __global__ void k_scale_copy(const float *in, float *out, size_t n, float sc)
 // Energy gate: the forcing F changes the energy at the rate P = sum w Re(conj(om/K^2) F); the
 // resolved energy of an unforced step can only fall (dE/dt = -2 nu Z), so the closure is kept
 // for this step only when P <= 2 nu Z, otherwise the step runs as the plain coarse step.
-// Grid kGateBlocks x 256: per-block partials, summed in block order by the last block to arrive.
-constexpr int kGateBlocks = 64;
+// Grid kGateBlocks x 256: per-block partials, summed by a fixed tree in the last block to arrive.
+constexpr int kGateBlocks = 64;  // <= the gate's 256 threads per block (one partial each in the last block)
 // scale == 0: the forcing is dropped (gate 0) for a step whose energy input P exceeds the viscous
 // loss 2 nu Z; scale == 1: it is scaled by 2 nu Z / P so that its input equals the loss
 __global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, int scale, float *gate,
@@ -3136,13 +3136,23 @@ __global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, fl
         last = (atomicAdd(counter, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        double Ps = 0.0, Zs = 0.0;
-        for (int b = 0; b < (int)gridDim.x; ++b) {
-            const double2 q = __ldcg(&part[b]);
-            Ps += q.x;
-            Zs += q.y;
+    if (!last) return;
+    // the last block sums the partials: one per thread, then the same tree (a single thread's
+    // loop over them waited out one L2 round trip after another)
+    double2 q = make_double2(0.0, 0.0);
+    if ((int)threadIdx.x < (int)gridDim.x) q = __ldcg(&part[threadIdx.x]);
+    sp[threadIdx.x] = q.x;
+    sz[threadIdx.x] = q.y;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+            sz[threadIdx.x] += sz[threadIdx.x + o];
         }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double Ps = sp[0], Zs = sz[0];
         *counter = 0u;
         const double loss = 2.0 * (double)visc * Zs;
         const bool keep = Ps <= loss;  // P > loss >= 0 below: the ratio is in [0, 1)
