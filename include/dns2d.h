@@ -227,6 +227,23 @@ int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed,
 /* The same forward on the BF16 tensor-core path: every layer runs as an implicit GEMM on tcgen05
  * (bf16 inputs, weights and activations, FP32 accumulation, GELU in its tanh form).  Needs channels == 32, layers >= 3 and W % 128 == 0 (DNS2D_ERR_SIZE otherwise). */
 int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, float *y);
+/* How the tensor-core path launches layers 1 .. L-1: mode 1 (default) one persistent,
+ * warp-specialised launch (one CTA per SM; tiles handed out in layer order, each waiting for its
+ * three input tile rows of the previous layer) wherever the weights of those layers fit in shared
+ * memory (layers <= 8), else one launch per layer; mode 0 always one launch per layer.  Both give
+ * the same values bit for bit.  tc_info reports the mode and the grid of the last persistent
+ * launch (0 before any). */
+int dns2d_cnn_set_tc_mode(dns2d_cnn *n, int mode);
+int dns2d_cnn_tc_info(const dns2d_cnn *n, int *mode, int *grid);
+/* Per-tile timestamps of the persistent launch (globaltimer ns; off by default): with tracing on,
+ * each persistent launch records for every tile (layer-major order, tile rows rotated by one per
+ * layer) 8 times: the producer took the tile, found its input rows complete, found its halo stage
+ * free, issued its copies; the MMA issuer found the copies landed, found the accumulator buffer
+ * free and issued the MMAs; the epilogue started, and its first warp released the tile (or wrote
+ * the output).  read_trace copies up to cap tiles x 8 values of the last launch and sets *tiles
+ * to its tile count. */
+int dns2d_cnn_set_trace(dns2d_cnn *n, int on);
+int dns2d_cnn_read_trace(dns2d_cnn *n, unsigned long long *out, int cap, int *tiles);
 
 /* Couple a trained network to a state as its subgrid closure (NULL network detaches): every
  * dns2d_step evaluates it on (omega/s0, u/s1, w/s2) of the current field on the L x L grid and

@@ -44,12 +44,13 @@ SYMBOLS = [
     "dns2d_cnn_set_dataset", "dns2d_cnn_train", "dns2d_closure_attach", "dns2d_closure_forcing", "dns2d_closure_stats",
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
     "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare", "dns2d_batch_prepare", "dns2d_batch_set_mode",
-    "dns2d_batch_set_waits", "dns2d_batch_set_items",
+    "dns2d_batch_set_waits", "dns2d_batch_set_items", "dns2d_cnn_set_tc_mode", "dns2d_cnn_tc_info",
+    "dns2d_cnn_set_trace", "dns2d_cnn_read_trace",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # translation units of libdns2d.so: the C ABI and one unit per group of compiled grid sizes
-SOURCES = ["dns2d_api.cu", "ensemble.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
+SOURCES = ["dns2d_api.cu", "ensemble.cu", "cnn_net.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
            "sets_29400.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]
@@ -175,6 +176,10 @@ def lib():
         "dns2d_closure_attach": (C.c_int, [vp, vp, fp, C.c_int]),
         "dns2d_closure_forcing": (C.c_int, [vp, fp]),
         "dns2d_cnn_forward_tc": (C.c_int, [vp, fp, C.c_int, C.c_int, C.c_int, fp]),
+        "dns2d_cnn_set_tc_mode": (C.c_int, [vp, C.c_int]),
+        "dns2d_cnn_tc_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "dns2d_cnn_set_trace": (C.c_int, [vp, C.c_int]),
+        "dns2d_cnn_read_trace": (C.c_int, [vp, C.POINTER(C.c_uint64), C.c_int, C.POINTER(C.c_int)]),
         "dns2d_closure_tensor_cores": (C.c_int, [vp, C.c_int]),
         "dns2d_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
         "dns2d_set_tuning": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
@@ -611,6 +616,33 @@ class CNN:
         y = np.zeros((B, 1, H, W), dtype=np.float32)
         self._chk(self._L.dns2d_cnn_forward_tc(self._n, _fp(x), B, H, W, _fp(y)))
         return y
+
+    def set_tc_mode(self, mode: int):
+        """1 (default): layers 1 .. L-1 of the tensor-core path in one persistent launch where their
+        weights fit in shared memory; 0: one launch per layer (same values bit for bit)."""
+        self._chk(self._L.dns2d_cnn_set_tc_mode(self._n, int(mode)))
+
+    def set_trace(self, on: bool):
+        """Record per-tile timestamps in each persistent launch (off by default)."""
+        self._chk(self._L.dns2d_cnn_set_trace(self._n, int(bool(on))))
+
+    def read_trace(self) -> np.ndarray:
+        """[tiles, 8] uint64 ns of the last persistent launch (tiles in layer order, tile rows
+        rotated by one per layer): taken, input rows complete, stage free, copies issued, copies
+        landed, MMAs issued, epilogue started, released."""
+        tiles = C.c_int(0)
+        self._chk(self._L.dns2d_cnn_read_trace(self._n, (C.c_uint64 * 1)(), 0, C.byref(tiles)))
+        out = np.zeros((tiles.value, 8), dtype=np.uint64)
+        if tiles.value:
+            self._chk(self._L.dns2d_cnn_read_trace(self._n, out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                   tiles.value, C.byref(tiles)))
+        return out
+
+    def tc_info(self):
+        """(mode, grid of the last persistent launch; 0 before any)."""
+        m, g = C.c_int(0), C.c_int(0)
+        self._chk(self._L.dns2d_cnn_tc_info(self._n, C.byref(m), C.byref(g)))
+        return m.value, g.value
 
     def loss_grad(self, x: np.ndarray, t: np.ndarray):
         x = np.ascontiguousarray(x, dtype=np.float32)

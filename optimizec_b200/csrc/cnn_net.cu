@@ -1,0 +1,386 @@
+// cnn_net.cu — the persistent, warp-specialised network launch (cnn_net.cuh): device roles and
+// the cooperative host launch.
+#include "cnn_net.cuh"
+
+#include <algorithm>
+
+namespace dns2d {
+namespace cnntc {
+namespace {
+
+__device__ __forceinline__ void mbar_init(uint64_t *m, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *m, uint32_t count = 1)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(saddr(m)), "r"(count)
+                 : "memory");
+}
+
+// one arrival that also announces the bytes the stage's bulk copies will deliver
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(saddr(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing on m
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *m)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(saddr(m))
+                 : "memory");
+}
+
+// orders this thread's generic-proxy view of global memory with its async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+
+struct Item {
+    int l, b, t, xs;
+};
+
+__device__ __forceinline__ Item decode(int item, int B, int T, int S)
+{
+    const int per_layer = B * T * S;
+    Item it;
+    const int j = item / per_layer;
+    int r = item - j * per_layer;
+    it.l = j + 1;
+    it.b = r / (T * S);
+    r -= it.b * (T * S);
+    const int pos = r / S;
+    it.xs = r - pos * S;
+    it.t = (pos + j) % T;  // layer l starts at tile row l - 1
+    return it;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Lanes 0, 1, 2 of the calling warp wait for the counters of tile rows t - 1, t, t + 1 of layer
+// l - 1 (every strip releases into them) to reach `need`; false when the wait ran out or another
+// wait did (recorded in *err).
+__device__ bool net_deps(const NetLaunch &q, const Item &it, int T, unsigned int need, int lane)
+{
+    const unsigned int *c = lane < 3 ? q.sync + 1 + ((size_t)(it.l - 2) * q.B + it.b) * T + (it.t + lane - 1 + T) % T
+                                     : nullptr;
+    long long n = 0;
+    for (;;) {
+        const bool ok = c == nullptr || ld_acquire_u32(c) >= need;
+        if (__all_sync(0xffffffffu, ok)) break;
+        const int e = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)q.err : 0, 0);
+        if (e != 0) return false;
+        if (++n > q.spin_limit) {
+            if (lane == 0) atomicExch(q.err, 1);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    __syncwarp();  // the lanes' acquires are ordered before lane 0's copies
+    return true;
+}
+
+// optional per-tile timestamps (globaltimer ns): producer [0] took the tile, [1] its input
+// rows complete, [2] its stage free, [3] copies issued; MMA issuer [4] copies landed, [5]
+// accumulator buffer free, MMAs issued; epilogue [6] started, [7] warp 0 of the tile's group
+// released it (or wrote its output)
+__device__ __forceinline__ void trace_at(const NetLaunch &q, int item, int j)
+{
+    if (q.trace) q.trace[(size_t)item * kNetTraceSlots + j] = global_ns();
+}
+
+// an epilogue warp's release of its share of a finished tile row (its stores were issued before)
+__device__ __forceinline__ void net_release(const NetLaunch &q, int idx, int lane)
+{
+    fence_proxy_async_global();
+    __syncwarp();
+    if (lane == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(q.sync + idx) : "memory");
+}
+
+// the 36 MMAs of one tile: output rows rr = 0, 1 into columns NO rr of the accumulator at d0;
+// descriptors built once (the 14-bit start-address field cannot carry: shared memory < 256 KB)
+template <int NO>
+__device__ __forceinline__ void issue_tile(uint32_t d0, uint32_t a0, uint32_t b0)
+{
+    const uint64_t da = smem_desc(a0, PLANE, 128), db = smem_desc(b0, NO * 16, 128);
+    constexpr uint32_t idesc = TcShape<NO>::IDESC;
+#pragma unroll
+    for (int rr = 0; rr < TR; ++rr)
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                mma_bf16(d0 + (uint32_t)(NO * rr), da + (uint64_t)(((2 * h) * PLANE + ((rr + t / 3) * HW + t % 3) * 16) >> 4),
+                         db + (uint64_t)(((t * 4 + 2 * h) * NO * 16) >> 4), idesc, (t | h) ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constant__ NetLaunch q)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t full[kNetMaxStages], empty[kNetMaxStages], tfull[kNetBufs], tempty[kNetBufs], wbar;
+    __shared__ int info[kNetMaxStages], tinfo[kNetBufs];
+    __shared__ uint32_t tmem_holder;
+    __shared__ int s_last;
+    __shared__ float sbias[kNetMaxLayers][C];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int L = q.L, NS = q.stages;
+    const int T = q.H / TR, S = q.W / TM;
+    const int total = (L - 1) * q.B * T * S;
+    unsigned char *sW = sm;                          // weights of layers 1 .. L-1
+    unsigned char *sStage = sm + net_weight_bytes(L);  // NS halo stages of A_BYTES
+
+    for (int e = tid; e < (L - 1) * C; e += kNetThreads) {
+        const int l = 1 + e / C, co = e % C;
+        sbias[l][co] = (l < L - 1 || co == 0) ? q.bias[l][co] : 0.0f;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(&tmem_holder)),
+                     "r"(kNetTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);   // the producer's expect_tx arrival + the copies' bytes
+            mbar_init(&empty[s], 1);  // the MMA commit of the stage's tile
+        }
+        for (int b = 0; b < kNetBufs; ++b) {
+            mbar_init(&tfull[b], 2);              // the MMA commit + the issuer's arrival (tile number)
+            mbar_init(&tempty[b], kNetGroupWarps);  // one arrival per warp of the tile's group
+        }
+        mbar_init(&wbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_holder;
+
+    if (warp == kNetEpiWarps) {
+        // ---------------- producer: tiles blockIdx.x, + gridDim.x, ... in increasing order ----------------
+        if (lane == 0) {
+            mbar_expect_tx(&wbar, (uint32_t)net_weight_bytes(L));
+            for (int l = 1; l < L; ++l) {
+                const size_t off = (size_t)(l - 1) * kNetWHidden;
+                bulk_g2s(sW + off, reinterpret_cast<const unsigned char *>(q.wtc) + off,
+                         l < L - 1 ? kNetWHidden : kNetWLast, &wbar);
+            }
+        }
+        const size_t plane = act_plane_px(q.H, q.W);  // 16-byte pixels per chunk plane
+        const size_t Wp = (size_t)q.W + 2;
+        const unsigned int need = (unsigned int)(kNetGroupWarps * S);
+        int k = 0;
+        for (;; ++k) {
+            const int s = k % NS;
+            int item = (int)blockIdx.x + k * (int)gridDim.x;
+            if (item >= total) item = -1;
+            Item it{};
+            if (item >= 0) {
+                if (lane == 0) trace_at(q, item, 0);
+                it = decode(item, q.B, T, S);
+                if (it.l >= 2 && !net_deps(q, it, T, need, lane)) item = -1;
+            }
+            if (lane == 0) {
+                if (item >= 0) trace_at(q, item, 1);
+                // the stage's previous tile (k - NS) has been read by its MMAs, so its phase of
+                // full[s] is complete (also before an end marker's arrival); if that wait runs
+                // out, nothing more arrives on full[s] and the issuer's own wait runs out
+                bool free = true;
+                if (k >= NS && !mbar_wait(&empty[s], (uint32_t)((k / NS - 1) & 1))) {
+                    atomicExch(q.err, 1);
+                    item = -1;
+                    free = false;
+                }
+                info[s] = item;
+                if (item < 0) {
+                    if (free) mbar_arrive(&full[s]);  // end marker
+                } else {
+                    trace_at(q, item, 2);
+                    fence_proxy_async_global();
+                    mbar_expect_tx(&full[s], (uint32_t)kNetHaloTx);
+                    // padded rows t TR .. t TR + TR + 1, padded pixels 128 xs .. 128 xs + 129
+                    const uint4 *src = reinterpret_cast<const uint4 *>(q.act[(it.l - 1) & 1]) +
+                                       (size_t)it.b * 4 * plane + (size_t)(it.t * TR) * Wp + (size_t)it.xs * TM;
+                    unsigned char *dst = sStage + (size_t)s * A_BYTES;
+                    for (int c = 0; c < 4; ++c)
+                        for (int r = 0; r < TR + 2; ++r)
+                            bulk_g2s(dst + c * PLANE + r * HW * 16, src + c * plane + (size_t)r * Wp, HW * 16,
+                                     &full[s]);
+                    trace_at(q, item, 3);
+                }
+            }
+            if (__shfl_sync(0xffffffffu, item, 0) < 0) break;
+        }
+        if (lane == 0) {
+            // copies still in flight: the last fill of each stage, and the weights (bounded waits)
+            for (int kk = (k - NS + 1 > 0 ? k - NS + 1 : 0); kk < k; ++kk)
+                mbar_wait(&full[kk % NS], (uint32_t)((kk / NS) & 1));
+            mbar_wait(&wbar, 0);
+        }
+        __syncwarp();
+    } else if (warp == kNetEpiWarps + 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            bool ok = mbar_wait(&wbar, 0);
+            if (!ok) atomicExch(q.err, 1);
+            const uint32_t w0 = saddr(sW), st0 = saddr(sStage);
+            const int per_layer = q.B * T * S;
+            int k = 0, last_k = -1;
+            for (;; ++k) {
+                const int s = k % NS, bb = k % kNetBufs;
+                int item = -1;
+                if (ok) {
+                    if (mbar_wait(&full[s], (uint32_t)((k / NS) & 1))) {
+                        item = info[s];
+                        if (item >= 0) trace_at(q, item, 4);
+                    } else {
+                        atomicExch(q.err, 1);
+                        ok = false;
+                    }
+                }
+                // the accumulator buffer's previous tile (k - 4) has been read by its epilogue
+                // group, so its phase of tfull[bb] is complete (also before an end marker's
+                // arrivals); if that wait runs out, nothing more arrives and the group's own wait
+                // runs out
+                if (k >= kNetBufs && !mbar_wait(&tempty[bb], (uint32_t)((k / kNetBufs - 1) & 1))) {
+                    atomicExch(q.err, 1);
+                    break;
+                }
+                tinfo[bb] = item;
+                if (item < 0) {
+                    // end markers for both epilogue groups (tiles k and k + 1)
+                    mbar_arrive(&tfull[bb], 2);
+                    const int k1 = k + 1, b1 = k1 % kNetBufs;
+                    if (k1 < kNetBufs || mbar_wait(&tempty[b1], (uint32_t)((k1 / kNetBufs - 1) & 1))) {
+                        tinfo[b1] = -1;
+                        mbar_arrive(&tfull[b1], 2);
+                    } else {
+                        atomicExch(q.err, 1);
+                    }
+                    break;
+                }
+                trace_at(q, item, 5);
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const int l = 1 + item / per_layer;
+                const uint32_t a0 = st0 + (uint32_t)(s * A_BYTES), b0 = w0 + (uint32_t)((l - 1) * kNetWHidden);
+                const uint32_t d0 = tmem + (uint32_t)(bb * TR * C);
+                if (l == L - 1)
+                    issue_tile<16>(d0, a0, b0);
+                else
+                    issue_tile<32>(d0, a0, b0);
+                mma_commit(&empty[s]);   // the stage may be refilled once these MMAs are done
+                mma_commit(&tfull[bb]);  // the accumulator is complete once these MMAs are done
+                mbar_arrive(&tfull[bb]);
+                last_k = k;
+            }
+            // MMAs still in flight: the last tile's commit (bounded wait)
+            if (last_k >= 0) mbar_wait(&empty[last_k % NS], (uint32_t)((last_k / NS) & 1));
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue: two groups of 8 warps take alternate tiles; in a group, warp
+        // w reads lanes 32 (w % 4) .. + 31 (pixels) x 32 columns (channels) of tile row (w / 4) % 2
+        const int grp = warp / kNetGroupWarps, qd = warp & 3, rr = (warp >> 2) & 1;
+        for (int k = grp;; k += 2) {
+            const int bb = k % kNetBufs;
+            const bool got = mbar_wait(&tfull[bb], (uint32_t)((k / kNetBufs) & 1));
+            if (!__all_sync(0xffffffffu, got)) {
+                if (lane == 0) atomicExch(q.err, 1);
+                break;
+            }
+            const int item = tinfo[bb];
+            if (item < 0) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const bool tr = (warp % kNetGroupWarps) == 0 && lane == 0;
+            if (tr) trace_at(q, item, 6);
+            const Item it = decode(item, q.B, T, S);
+            const int y = it.t * TR + rr, x = it.xs * TM + qd * 32 + lane;
+            const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(bb * TR * C);
+            if (it.l < L - 1) {
+                uint32_t r[32];
+                tmem_ld32(taddr + (uint32_t)(C * rr), r);
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[bb]);
+                uint4 v[4];
+                gelu_chunks(r, sbias[it.l], v);
+                store_px(q.act[it.l & 1], it.b, q.H, q.W, y, x, v);
+                net_release(q, 1 + (int)(((size_t)(it.l - 1) * q.B + it.b) * T + it.t), lane);
+            } else {
+                uint32_t r0;
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n"
+                             : "=r"(r0)
+                             : "r"(taddr + (uint32_t)(16 * rr)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[bb]);
+                q.yf[((size_t)it.b * q.H + y) * q.W + x] = (__uint_as_float(r0) + sbias[it.l][0]) * q.out_scale;
+            }
+            if (tr) trace_at(q, item, 7);
+        }
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kNetTmemCols));
+    // the last CTA to finish resets the counters for the next launch
+    if (tid == 0) {
+        __threadfence();
+        s_last = (atomicAdd(q.sync, 1u) == gridDim.x - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        const size_t n = net_sync_words(L, q.B, q.H);
+        for (size_t i = tid; i < n; i += kNetThreads) q.sync[i] = 0u;
+    }
+}
+
+}  // namespace
+
+int net_stages_that_fit(int L)
+{
+    if (L < 3 || L > kNetMaxLayers) return 0;
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa{};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, k_cnn_net) != cudaSuccess)
+        return 0;
+    for (int s = kNetMaxStages; s >= 2; --s)
+        if (net_smem_bytes(L, s) + fa.sharedSizeBytes <= (size_t)optin) return s;
+    return 0;
+}
+
+// One CTA per SM (the shared memory holds one), no more than there are tiles; a cooperative
+// launch, which the driver refuses rather than run with CTAs that are not all resident.
+cudaError_t net_launch(const NetLaunch &q, cudaStream_t stream, int *grid_out)
+{
+    const size_t smem = net_smem_bytes(q.L, q.stages);
+    cudaError_t e = cudaFuncSetAttribute(k_cnn_net, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cnn_net, kNetThreads, smem)) != cudaSuccess)
+        return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const long long items = (long long)(q.L - 1) * q.B * (q.H / TR) * (q.W / TM);
+    const int grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm, items));
+    if (grid_out) *grid_out = grid;
+    void *args[] = {const_cast<NetLaunch *>(&q)};
+    return cudaLaunchCooperativeKernel((void *)k_cnn_net, grid, kNetThreads, args, smem, stream);
+}
+
+}  // namespace cnntc
+}  // namespace dns2d

@@ -4,15 +4,18 @@
 // tensor cores: D[128 pixels][32 co] += A[128 pixels][16 ci] B[16 ci][32 co], 18 MMAs per tile
 // (9 taps x 2 halves of the 32 input channels), FP32 accumulation in tensor memory.
 //
-// Activations are NHWC bf16 (64 bytes per pixel).  A CTA owns 128 consecutive pixels of TR = 2 image
-// rows; it stages the 4-row, 130-pixel halo in shared memory as 4 planes of 16-byte channel chunks
-// (plane c holds channels 8c..8c+7 of every halo pixel, 16 bytes per pixel).  In that layout the
-// A operand of tap (dy, dx) is the same K-major "no swizzle" canonical tile (8-pixel core matrices
-// 128 bytes apart, the two K chunks one plane apart) started at another 16-byte address, so the 9
-// taps need no data movement.  The weights are staged as [tap][chunk][co][8 ci] bf16.
-// One thread issues the MMAs and commits them to an mbarrier; the 4 warps then read their 32 TMEM
-// lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.  The
-// last layer (32 -> 1) is the same kernel with N = 16 (15 zero weight columns) writing channel 0
+// Activations are bf16 in a padded chunk-planar layout: per image 4 planes (plane c holds channels
+// 8c..8c+7 of every pixel, 16 bytes per pixel), each (H + 2) x (W + 2) pixels with a one-pixel
+// periodic frame (padded pixel (y + 1, x + 1) is image pixel (y, x); frame rows and columns hold
+// the periodic neighbours, written by the producing layer's epilogue).  A CTA owns 128
+// consecutive pixels of TR = 2 image rows; its 4-row, 130-pixel halo is then one contiguous
+// 2080-byte run per (plane, row), copied unchanged into shared memory as 4 chunk planes.  In that
+// layout the A operand of tap (dy, dx) is the same K-major "no swizzle" canonical tile (8-pixel
+// core matrices 128 bytes apart, the two K chunks one plane apart) started at another 16-byte
+// address, so the 9 taps need no data movement.  The weights are staged as [tap][chunk][co][8 ci]
+// bf16.  One thread issues the MMAs and commits them to an mbarrier; the warps then read their 32
+// TMEM lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.  The
+// last layer (32 -> 1) is the same MMA with N = 16 (15 zero weight columns) writing channel 0
 // in FP32 times the output scale.  The first layer (3 -> 32) builds its A operand as an im2col
 // tile in shared memory (K = 3 channels x 9 taps = 27, padded to 32) straight from the three FP32
 // input planes times their input scales: 2 MMAs per tile.
@@ -47,7 +50,14 @@ struct TcShape {
     static constexpr uint32_t IDESC =
         (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NO >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 };
-constexpr unsigned kWaitLimit = 1u << 22;        // mbarrier polls before giving up
+constexpr unsigned long long kWaitNs = 2000000000ull;  // an mbarrier wait gives up after 2 s
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // UMMA shared-memory descriptor, K-major, no swizzle (version 1 = sm_100 format)
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
@@ -71,6 +81,33 @@ __device__ __forceinline__ float gelu_f(float z)
 
 // periodic index in [0, n) of i in [-n, 2n)
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// padded chunk-planar activations: 16-byte pixels per plane, 4 planes per image
+__host__ __device__ __forceinline__ size_t act_plane_px(int H, int W) { return (size_t)(H + 2) * (W + 2); }
+__host__ __device__ __forceinline__ size_t act_bytes(int B, int H, int W) { return (size_t)B * 4 * act_plane_px(H, W) * 16; }
+
+// the 4 chunks of image pixel (y, x) of image b, at its padded position and at every frame
+// position that repeats it (H >= 2, W >= 2)
+__device__ __forceinline__ void store_px(__nv_bfloat16 *act, int b, int H, int W, int y, int x, const uint4 (&v)[4])
+{
+    const size_t plane = act_plane_px(H, W), Wp = (size_t)W + 2;
+    uint4 *base = reinterpret_cast<uint4 *>(act) + (size_t)b * 4 * plane;
+    const int py1 = y == 0 ? H + 1 : (y == H - 1 ? 0 : -1);
+    const int px1 = x == 0 ? W + 1 : (x == W - 1 ? 0 : -1);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int py = i == 0 ? y + 1 : py1;
+        if (py < 0) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int px = j == 0 ? x + 1 : px1;
+            if (px < 0) continue;
+            uint4 *d = base + (size_t)py * Wp + px;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) d[c * plane] = v[c];
+        }
+    }
+}
 
 // weights of a 32 -> Co layer, w[co][ci][3][3] f32 -> wtc[tap][chunk][NO][8] bf16 (co >= Co zero)
 template <int NO>
@@ -128,19 +165,28 @@ __device__ __forceinline__ void mma_commit(uint64_t *mbar)
                  : "memory");
 }
 
-// bounded wait for phase 0 of the mbarrier; false when the limit ran out
-__device__ __forceinline__ bool mma_wait(uint64_t *mbar)
+// wait (at most kWaitNs) for the phase of the given parity to complete; false when it ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity)
 {
     uint32_t done = 0;
-    for (unsigned it = 0; it < kWaitLimit && !done; ++it) {
+    const unsigned long long t0 = global_ns();
+    for (;;) {
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(saddr(mbar)), "r"(0u)
+            : "r"(saddr(mbar)), "r"(parity)
             : "memory");
+        if (done || global_ns() - t0 > kWaitNs) break;
     }
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     return done != 0;
+}
+
+// bounded wait for phase 0 of the mbarrier; false when the limit ran out
+__device__ __forceinline__ bool mma_wait(uint64_t *mbar)
+{
+    const bool done = mbar_wait(mbar, 0u);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    return done;
 }
 
 template <int COLS>
@@ -152,10 +198,22 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem_d)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_d), "r"(COLS));
 }
 
-// 32 accumulator columns of this warp's 32 lanes -> bias, GELU, bf16, 64-byte store of one pixel
-__device__ __forceinline__ void epilogue32(uint32_t taddr, const float *__restrict__ bias, __nv_bfloat16 *dstpix)
+// 32 accumulator columns (already loaded) -> bias, GELU, bf16: the pixel's 4 chunks
+__device__ __forceinline__ void gelu_chunks(const uint32_t (&r)[32], const float *bias, uint4 (&v)[4])
 {
-    uint32_t r[32];
+    __align__(16) __nv_bfloat162 o[C / 2];
+#pragma unroll
+    for (int co = 0; co < C; co += 2)
+        o[co / 2] = __floats2bfloat162_rn(gelu_f(__uint_as_float(r[co]) + bias[co]),
+                                          gelu_f(__uint_as_float(r[co + 1]) + bias[co + 1]));
+    const uint4 *src = reinterpret_cast<const uint4 *>(o);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = src[q];
+}
+
+// 32 consecutive accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
@@ -165,21 +223,23 @@ __device__ __forceinline__ void epilogue32(uint32_t taddr, const float *__restri
           "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    __align__(16) __nv_bfloat162 o[C / 2];
-#pragma unroll
-    for (int co = 0; co < C; co += 2)
-        o[co / 2] = __floats2bfloat162_rn(gelu_f(__uint_as_float(r[co]) + bias[co]),
-                                          gelu_f(__uint_as_float(r[co + 1]) + bias[co + 1]));
-    uint4 *dst = reinterpret_cast<uint4 *>(dstpix);
-    const uint4 *src = reinterpret_cast<const uint4 *>(o);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = src[q];
+}
+
+// this warp's 32 lanes x 32 columns -> bias, GELU, bf16 pixel (y, x) of image b in the padded layout
+__device__ __forceinline__ void epilogue32(uint32_t taddr, const float *__restrict__ bias, __nv_bfloat16 *act, int b,
+                                           int H, int W, int y, int x)
+{
+    uint32_t r[32];
+    tmem_ld32(taddr, r);
+    uint4 v[4];
+    gelu_chunks(r, bias, v);
+    store_px(act, b, H, W, y, x, v);
 }
 
 // ------------------------------------------------------------------------------------------
 // 32 -> NO layer.  Grid (W/128 * H/TR, B), 128 threads; W % 128 == 0, H % TR == 0.
-// NO = 32: GELU, bf16 NHWC output y.  NO = 16: channel 0 times out_scale, f32 output yf
-// ([B][H][W], no activation).
+// Input x and output y in the padded chunk-planar layout.  NO = 32: GELU, bf16 output y.  NO = 16:
+// channel 0 times out_scale, f32 output yf ([B][H][W], no activation).
 // ------------------------------------------------------------------------------------------
 template <int NO>
 __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict__ x,
@@ -201,13 +261,14 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
     const int x0 = (blockIdx.x % tiles_x) * TM;
     const size_t img = (size_t)blockIdx.y * H * W;
 
-    // halo: rows y0-1..y0+TR, pixels x0-1..x0+128 (periodic), 4 chunks of 16 bytes each; pixel-major
-    // so that a warp copies 8 whole pixels (512 contiguous bytes)
-    for (int e = tid; e < (TR + 2) * HW * 4; e += NT) {
-        const int r = e >> 2, c = e & 3;
+    // halo: padded rows y0 .. y0 + TR + 1, padded pixels x0 .. x0 + 129 of each chunk plane; a warp
+    // copies 32 consecutive 16-byte pixels (512 contiguous bytes)
+    const size_t plane = act_plane_px(H, W);
+    const uint4 *xin = reinterpret_cast<const uint4 *>(x) + (size_t)blockIdx.y * 4 * plane;
+    for (int e = tid; e < 4 * (TR + 2) * HW; e += NT) {
+        const int c = e / ((TR + 2) * HW), r = e - c * ((TR + 2) * HW);
         const int row = r / HW, xi = r - row * HW;
-        const int sy = wrap(y0 - 1 + row, H), sx = wrap(x0 - 1 + xi, W);
-        cp16(sA + c * PLANE + r * 16, x + ((img + (size_t)sy * W + sx) * C + c * 8));
+        cp16(sA + c * PLANE + r * 16, xin + c * plane + (size_t)(y0 + row) * (W + 2) + x0 + xi);
     }
     for (int e = tid; e < B_BYTES / 16; e += NT) cp16(sB + e * 16, wtc + (size_t)e * 8);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -236,7 +297,7 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
             const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(NO * rr);
             const size_t pix = img + (size_t)(y0 + rr) * W + x0 + m;
             if constexpr (NO == 32) {
-                epilogue32(taddr, bias, y + pix * C);
+                epilogue32(taddr, bias, y, blockIdx.y, H, W, y0 + rr, x0 + m);
             } else {
                 uint32_t r0;
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(r0) : "r"(taddr));
@@ -254,7 +315,8 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
 // 3 -> 32 layer on the tensor cores: K = 27 (channel ci, tap ky, kx at k = 9 ci + 3 ky + kx),
 // padded to 32.  The inputs are three f32 planes p[c] (image b at p[c] + b * pstride) times
 // s[c]; the im2col tile of TR rows x 128 pixels is built in shared memory as 4 chunk planes of
-// [pixel][8 k] bf16.  Weights [chunk][32 co][8 k] bf16 (k >= 27 zero).  GELU, bf16 NHWC output.
+// [pixel][8 k] bf16.  Weights [chunk][32 co][8 k] bf16 (k >= 27 zero).  GELU, bf16 output in the
+// padded chunk-planar layout.
 // ------------------------------------------------------------------------------------------
 struct FirstIn {
     const float *p[3];
@@ -266,7 +328,7 @@ constexpr int B_FIRST = 4 * C * 16;          // 2 KB of weights
 constexpr int SMEM_FIRST = 4 * PLANE_F + B_FIRST;
 
 // w0[co][ci][3][3] f32 -> [chunk][co][8] bf16
-__global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wtc)
+static __global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wtc)
 {
     for (int e = threadIdx.x; e < 4 * C * 8; e += blockDim.x) {
         const int ch = e / (C * 8), r = e % (C * 8), co = r / 8, k = ch * 8 + r % 8;
@@ -274,7 +336,7 @@ __global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *__restr
     }
 }
 
-__global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const __nv_bfloat16 *__restrict__ wtc,
+static __global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const __nv_bfloat16 *__restrict__ wtc,
                                                       const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
                                                       int H, int W, int *__restrict__ err)
 {
@@ -333,7 +395,7 @@ __global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const __nv_bfl
 #pragma unroll 1
         for (int rr = 0; rr < TR; ++rr) {
             const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(C * rr);
-            epilogue32(taddr, bias, y + (((size_t)b * H + y0 + rr) * W + x0 + m) * C);
+            epilogue32(taddr, bias, y, b, H, W, y0 + rr, x0 + m);
         }
     } else if (lane == 0) {
         atomicExch(err, 1);

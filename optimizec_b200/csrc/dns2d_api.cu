@@ -17,6 +17,7 @@
 #include "kernel_sets.cuh"
 #include "ensemble.cuh"
 #include "cnn.cuh"
+#include "cnn_net.cuh"
 #include "cnn_tc.cuh"
 #include "../../include/dns2d.h"
 
@@ -2653,12 +2654,21 @@ struct dns2d_cnn {
     long long step = 0;
     float *data_x = nullptr, *data_t = nullptr;  // device-resident training set
     int data_n = 0, data_H = 0, data_W = 0;
-    // BF16 tensor-core inference path (cnn_tc.cuh): packed hidden-layer weights, NHWC bf16
-    // activations, error flag of the bounded waits; gen counts parameter changes
+    // BF16 tensor-core inference path (cnn_tc.cuh, cnn_net.cuh): packed weights, padded
+    // chunk-planar bf16 activations, error flag of the bounded waits; gen counts parameter
+    // changes.  tc_mode 1 runs layers 1 .. L-1 as one persistent launch where their weights fit
+    // in shared memory (net_sync: its ticket and row counters), 0 one launch per layer.
     __nv_bfloat16 *wtc = nullptr;
     __nv_bfloat16 *act_tc[2] = {nullptr, nullptr};
-    size_t act_tc_cap = 0;
+    size_t act_tc_cap = 0;  // bytes of each activation buffer
     int *tc_err = nullptr;
+    unsigned int *net_sync = nullptr;
+    size_t net_sync_cap = 0;  // words
+    int tc_mode = 1, net_grid = 0;
+    // optional per-tile timestamps of the persistent launch (8 per tile, the last launch's)
+    unsigned long long *trace = nullptr;
+    size_t trace_cap = 0;  // tiles
+    int trace_on = 0, trace_tiles = 0;
     long long gen = 0, tc_gen = -1;
     std::string err;
 };
@@ -2748,7 +2758,7 @@ bool cnn_tc_supported(const dns2d_cnn *n, int H, int W)
 
 int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
 {
-    const size_t need = (size_t)B * H * W * dns2d::cnntc::C;
+    const size_t need = dns2d::cnntc::act_bytes(B, H, W);
     CNN_CUDA(cudaFuncSetAttribute(dns2d::cnntc::k_conv_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   dns2d::cnntc::TcShape<32>::SMEM_BYTES),
              "tc smem attribute");
@@ -2769,9 +2779,20 @@ int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
         cudaFree(n->act_tc[0]);
         cudaFree(n->act_tc[1]);
         n->act_tc[0] = n->act_tc[1] = nullptr;
-        CNN_CUDA(cudaMalloc((void **)&n->act_tc[0], need * 2), "tc activation alloc");
-        CNN_CUDA(cudaMalloc((void **)&n->act_tc[1], need * 2), "tc activation alloc");
+        CNN_CUDA(cudaMalloc((void **)&n->act_tc[0], need), "tc activation alloc");
+        CNN_CUDA(cudaMalloc((void **)&n->act_tc[1], need), "tc activation alloc");
         n->act_tc_cap = need;
+    }
+    // counters of the persistent launch: zero once, then reset by each launch's last CTA
+    const size_t words = dns2d::cnntc::net_sync_words(n->layers, B, H);
+    if (words > n->net_sync_cap) {
+        CNN_CUDA(cudaStreamSynchronize(n->stream), "sync");
+        cudaFree(n->net_sync);
+    cudaFree(n->trace);
+        n->net_sync = nullptr;
+        CNN_CUDA(cudaMalloc((void **)&n->net_sync, words * 4), "network counters alloc");
+        CNN_CUDA(cudaMemset(n->net_sync, 0, words * 4), "network counters clear");
+        n->net_sync_cap = words;
     }
     return DNS2D_OK;
 }
@@ -2803,6 +2824,38 @@ int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, const dns2d::cnntc::Fi
     const __nv_bfloat16 *w_first = w_last + 9 * 4 * 16 * 8;
     k_conv_tc_first<<<grid, NT, SMEM_FIRST, st>>>(in, w_first, n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
                                                   n->act_tc[0], H, W, n->tc_err);
+    const int stages = n->tc_mode == 1 ? net_stages_that_fit(L) : 0;
+    if (stages >= 2) {
+        NetLaunch q;
+        q.wtc = n->wtc;
+        for (int l = 1; l < L; ++l) q.bias[l] = n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9;
+        q.act[0] = n->act_tc[0];
+        q.act[1] = n->act_tc[1];
+        q.yf = n->z[L - 1];
+        q.out_scale = out_scale;
+        q.L = L;
+        q.B = B;
+        q.H = H;
+        q.W = W;
+        q.stages = stages;
+        q.sync = n->net_sync;
+        q.err = n->tc_err;
+        if (n->trace_on) {
+            const size_t tiles = (size_t)(L - 1) * B * (H / TR) * (W / TM);
+            if (tiles > n->trace_cap) {
+                CNN_CUDA(cudaStreamSynchronize(st), "sync");
+                cudaFree(n->trace);
+                n->trace = nullptr;
+                CNN_CUDA(cudaMalloc((void **)&n->trace, tiles * kNetTraceSlots * sizeof(unsigned long long)),
+                         "trace alloc");
+                n->trace_cap = tiles;
+            }
+            q.trace = n->trace;
+            n->trace_tiles = (int)tiles;
+        }
+        CNN_CUDA(net_launch(q, st, &n->net_grid), "persistent network launch");
+        return DNS2D_OK;
+    }
     int cur = 0;
     for (int l = 1; l + 1 < L; ++l) {
         const float *bias = n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9;
@@ -2881,6 +2934,8 @@ extern "C" void dns2d_cnn_destroy(dns2d_cnn *n)
     cudaFree(n->act_tc[0]);
     cudaFree(n->act_tc[1]);
     cudaFree(n->tc_err);
+    cudaFree(n->net_sync);
+    cudaFree(n->trace);
     if (n->stream) cudaStreamDestroy(n->stream);
     delete n;
 }
@@ -2969,6 +3024,42 @@ extern "C" int dns2d_cnn_forward(dns2d_cnn *n, const float *x, int B, int H, int
     if (rc) return rc;
     CNN_CUDA(cudaMemcpyAsync(y, n->z[n->layers - 1], (size_t)B * H * W * 4, cudaMemcpyDeviceToHost, n->stream), "out copy");
     CNN_CUDA(cudaStreamSynchronize(n->stream), "forward sync");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_set_tc_mode(dns2d_cnn *n, int mode)
+{
+    if (!n || mode < 0 || mode > 1) return DNS2D_ERR_ARG;
+    n->tc_mode = mode;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_set_trace(dns2d_cnn *n, int on)
+{
+    if (!n || on < 0 || on > 1) return DNS2D_ERR_ARG;
+    n->trace_on = on;
+    if (!on) n->trace_tiles = 0;
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_read_trace(dns2d_cnn *n, unsigned long long *out, int cap, int *tiles)
+{
+    if (!n || !out || cap < 0 || !tiles) return DNS2D_ERR_ARG;
+    *tiles = n->trace_tiles;
+    const int m = n->trace_tiles < cap ? n->trace_tiles : cap;
+    if (m <= 0) return DNS2D_OK;
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "trace sync");
+    CNN_CUDA(cudaMemcpy(out, n->trace, (size_t)m * dns2d::cnntc::kNetTraceSlots * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost),
+             "trace copy");
+    return DNS2D_OK;
+}
+
+extern "C" int dns2d_cnn_tc_info(const dns2d_cnn *n, int *mode, int *grid)
+{
+    if (!n) return DNS2D_ERR_ARG;
+    if (mode) *mode = n->tc_mode;
+    if (grid) *grid = n->net_grid;
     return DNS2D_OK;
 }
 

@@ -54,3 +54,68 @@ def test_tensor_core_path_rejects_unsupported_width():
     with pytest.raises(P().Dns2dError):
         net.forward_tc(np.zeros((1, 3, 8, 96), np.float32))
     net.close()
+
+
+@pytest.mark.parametrize("B,H,W,layers", [
+    (1, 384, 384, 6),  # the closure's N = 256 grid: 192 tile rows x 3 strips per layer
+    (2, 6, 128, 4),    # three tile rows: every row depends on all three rows of the layer before
+    (1, 4, 256, 5),    # two tile rows (the neighbours above and below are the same row)
+    (3, 2, 128, 3),    # one tile row and one hidden layer
+    (1, 8, 128, 8),    # the deepest network whose weights fit (three halo stages)
+])
+def test_persistent_launch_matches_per_layer_launches(B, H, W, layers):
+    """Layers 1 .. L-1 as one persistent, warp-specialised launch (tiles in layer order, each after
+    its three input tile rows) give the per-layer kernels' values bit for bit, call after call."""
+    rng = np.random.default_rng(11)
+    net = P().CNN(layers, 32, seed=7)
+    x = rng.standard_normal((B, 3, H, W)).astype(np.float32)
+    net.set_tc_mode(0)
+    y0 = net.forward_tc(x)
+    assert net.tc_info() == (0, 0)
+    net.set_tc_mode(1)
+    for _ in range(3):  # the counters reset by each launch's last CTA serve the next one
+        np.testing.assert_array_equal(net.forward_tc(x), y0)
+    mode, grid = net.tc_info()
+    assert mode == 1 and 0 < grid <= min(148, (layers - 1) * B * (H // 2) * (W // 128))
+    # both paths against the bf16 restatement (exact erf GELU; the kernels' tanh form and FP32
+    # accumulation order put this draw at 5.4e-3 at 384^2)
+    y_bf = forward_bf16(net.params(), layers, x)
+    assert np.linalg.norm(y0 - y_bf) <= 1e-2 * np.linalg.norm(y_bf)
+    net.close()
+
+
+def test_deep_network_runs_one_launch_per_layer():
+    """Nine layers are past the persistent launch's eight, so the persistent mode falls back to
+    one launch per layer (no persistent grid recorded)."""
+    rng = np.random.default_rng(12)
+    net = P().CNN(9, 32, seed=8)
+    x = rng.standard_normal((1, 3, 4, 128)).astype(np.float32)
+    y = net.forward_tc(x)
+    assert net.tc_info() == (1, 0)
+    net.set_tc_mode(0)
+    np.testing.assert_array_equal(net.forward_tc(x), y)
+    # nine bf16-rounded layers (the tanh GELU against the restatement's erf): 1.05e-2 for this draw
+    y_bf = forward_bf16(net.params(), 9, x)
+    assert np.linalg.norm(y - y_bf) <= 3e-2 * np.linalg.norm(y_bf)
+    net.close()
+
+
+def test_persistent_launch_trace():
+    """The per-tile timestamps of a traced persistent launch: every tile recorded, each tile's
+    eight events (taken, inputs complete, stage free, copies issued, copies landed, MMAs issued,
+    epilogue started, released) in that order, and tracing leaves the values alone."""
+    rng = np.random.default_rng(13)
+    net = P().CNN(6, 32, seed=9)
+    x = rng.standard_normal((1, 3, 64, 256)).astype(np.float32)
+    y0 = net.forward_tc(x)
+    assert net.read_trace().shape == (0, 8)
+    net.set_trace(True)
+    np.testing.assert_array_equal(net.forward_tc(x), y0)
+    tr = net.read_trace().astype(np.int64)
+    assert tr.shape == (5 * 32 * 2, 8)
+    assert (tr > 0).all()
+    assert (np.diff(tr, axis=1) >= 0).all()
+    # the first layer's tiles start before the last layer's end
+    assert tr[:64, 0].min() < tr[-64:, 7].max()
+    net.set_trace(False)
+    net.close()
