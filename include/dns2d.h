@@ -238,9 +238,9 @@ int dns2d_cnn_tc_info(const dns2d_cnn *n, int *mode, int *grid);
 /* Per-tile timestamps of the persistent launch (globaltimer ns; off by default): with tracing on,
  * each persistent launch records for every tile (layer-major order, tile rows rotated by one per
  * layer) 8 times: the producer took the tile, found its input rows complete, found its halo stage
- * free, issued its copies; the MMA issuer found the copies landed, found the accumulator buffer
- * free and issued the MMAs; the epilogue started, and its first warp released the tile (or wrote
- * the output).  read_trace copies up to cap tiles x 8 values of the last launch and sets *tiles
+ * free, issued its halo copy; the MMA issuer found the copy landed, then (once the accumulator
+ * buffer was free) had issued and committed the MMAs; the epilogue started, and its first warp
+ * released the tile (or wrote the output).  read_trace copies up to cap tiles x 8 values of the last launch and sets *tiles
  * to its tile count. */
 int dns2d_cnn_set_trace(dns2d_cnn *n, int on);
 int dns2d_cnn_read_trace(dns2d_cnn *n, unsigned long long *out, int cap, int *tiles);

@@ -627,12 +627,13 @@ class CNN:
         self._chk(self._L.dns2d_cnn_set_trace(self._n, int(bool(on))))
 
     def read_trace(self) -> np.ndarray:
-        """[tiles, 8] uint64 ns of the last persistent launch (tiles in layer order, tile rows
-        rotated by one per layer): taken, input rows complete, stage free, copies issued, copies
-        landed, MMAs issued, epilogue started, released."""
+        """[tiles, 10] uint64 ns of the last persistent launch (tiles in layer order, tile rows
+        rotated by one per layer): taken, input rows complete, stage free, copy issued, copy
+        landed, MMAs issued and committed, epilogue started, accumulator read, stores issued,
+        released."""
         tiles = C.c_int(0)
         self._chk(self._L.dns2d_cnn_read_trace(self._n, (C.c_uint64 * 1)(), 0, C.byref(tiles)))
-        out = np.zeros((tiles.value, 8), dtype=np.uint64)
+        out = np.zeros((tiles.value, 10), dtype=np.uint64)
         if tiles.value:
             self._chk(self._L.dns2d_cnn_read_trace(self._n, out.ctypes.data_as(C.POINTER(C.c_uint64)),
                                                    tiles.value, C.byref(tiles)))

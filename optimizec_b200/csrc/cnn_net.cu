@@ -65,61 +65,72 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
     return v;
 }
 
-// Lanes 0, 1, 2 of the calling warp wait for the counters of tile rows t - 1, t, t + 1 of layer
-// l - 1 (every strip releases into them) to reach `need`; false when the wait ran out or another
-// wait did (recorded in *err).
-__device__ bool net_deps(const NetLaunch &q, const Item &it, int T, unsigned int need, int lane)
+// Wait until tile `item` (and as many of the next kNetLookahead - 1 tiles of this CTA, every G
+// tiles, as are ready too) has its input rows complete: lanes 3j, 3j + 1, 3j + 2 read the
+// counters of tile rows t - 1, t, t + 1 of layer l - 1 for the tile j steps ahead (acquire loads;
+// every strip releases into them).  Returns how many consecutive tiles from `item` are ready
+// (>= 1), or 0 when the wait ran out or another wait did (recorded in *err).
+__device__ int net_deps(const NetLaunch &q, int item, int G, int total, int T, int S, unsigned int need, int lane)
 {
-    const unsigned int *c = lane < 3 ? q.sync + 1 + ((size_t)(it.l - 2) * q.B + it.b) * T + (it.t + lane - 1 + T) % T
-                                     : nullptr;
+    const int j = lane / 3, d = lane - 3 * (lane / 3);
+    const unsigned int *c = nullptr;
+    const int it_j = item + j * G;
+    if (j < kNetLookahead && it_j < total) {
+        const Item it = decode(it_j, q.B, T, S);
+        if (it.l >= 2) c = q.sync + 1 + ((size_t)(it.l - 2) * q.B + it.b) * T + (it.t + d - 1 + T) % T;
+    }
     long long n = 0;
     for (;;) {
         const bool ok = c == nullptr || ld_acquire_u32(c) >= need;
-        if (__all_sync(0xffffffffu, ok)) break;
+        const unsigned int mask = __ballot_sync(0xffffffffu, ok);
+        int m = 0;
+        while (m < kNetLookahead && ((mask >> (3 * m)) & 7u) == 7u) ++m;
+        if (m > 0) {
+            __syncwarp();  // the lanes' acquires are ordered before lane 0's copies
+            return m;
+        }
         const int e = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)q.err : 0, 0);
-        if (e != 0) return false;
+        if (e != 0) return 0;
         if (++n > q.spin_limit) {
             if (lane == 0) atomicExch(q.err, 1);
-            return false;
+            return 0;
         }
         __nanosleep(64);
     }
-    __syncwarp();  // the lanes' acquires are ordered before lane 0's copies
-    return true;
 }
 
 // optional per-tile timestamps (globaltimer ns): producer [0] took the tile, [1] its input
-// rows complete, [2] its stage free, [3] copies issued; MMA issuer [4] copies landed, [5]
-// accumulator buffer free, MMAs issued; epilogue [6] started, [7] warp 0 of the tile's group
-// released it (or wrote its output)
+// rows complete, [2] its stage free, [3] copy issued; MMA issuer [4] copy landed, [5] MMAs
+// issued and committed (after the accumulator buffer was free); warp 0 of the tile's epilogue
+// group [6] started, [7] read the accumulator, [8] issued its stores, [9] released the tile (or
+// wrote its output)
 __device__ __forceinline__ void trace_at(const NetLaunch &q, int item, int j)
 {
     if (q.trace) q.trace[(size_t)item * kNetTraceSlots + j] = global_ns();
 }
 
-// an epilogue warp's release of its share of a finished tile row (its stores were issued before)
-__device__ __forceinline__ void net_release(const NetLaunch &q, int idx, int lane)
+// AND of p over an epilogue group's 256 threads at its named barrier 1 + grp: the group takes
+// every decision together, so no warp of it can be left waiting at the group's barrier
+__device__ __forceinline__ bool group_all(bool p, int grp)
 {
-    fence_proxy_async_global();
-    __syncwarp();
-    if (lane == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(q.sync + idx) : "memory");
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(1 + grp), "r"(kNetGroupWarps * 32)
+        : "memory");
+    return r != 0;
 }
 
-// the 36 MMAs of one tile: output rows rr = 0, 1 into columns NO rr of the accumulator at d0;
-// descriptors built once (the 14-bit start-address field cannot carry: shared memory < 256 KB)
-template <int NO>
-__device__ __forceinline__ void issue_tile(uint32_t d0, uint32_t a0, uint32_t b0)
+// An epilogue group's release of a finished tile: every warp orders its stores for the async
+// proxy, the group meets at its named barrier (1 + grp, the group's 256 threads), and one thread
+// releases the tile-row counter (cumulative over the group's stores seen through the barrier).
+// The other warps go on to their next tile without waiting for the stores.
+__device__ __forceinline__ void net_release(const NetLaunch &q, int idx, int grp, bool leader)
 {
-    const uint64_t da = smem_desc(a0, PLANE, 128), db = smem_desc(b0, NO * 16, 128);
-    constexpr uint32_t idesc = TcShape<NO>::IDESC;
-#pragma unroll
-    for (int rr = 0; rr < TR; ++rr)
-#pragma unroll
-        for (int t = 0; t < 9; ++t)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                mma_bf16(d0 + (uint32_t)(NO * rr), da + (uint64_t)(((2 * h) * PLANE + ((rr + t / 3) * HW + t % 3) * 16) >> 4),
-                         db + (uint64_t)(((t * 4 + 2 * h) * NO * 16) >> 4), idesc, (t | h) ? 1u : 0u);
+    fence_proxy_async_global();
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(kNetGroupWarps * 32) : "memory");
+    if (leader) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(q.sync + idx) : "memory");
 }
 
 __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constant__ NetLaunch q)
@@ -135,8 +146,9 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
     const int L = q.L, NS = q.stages;
     const int T = q.H / TR, S = q.W / TM;
     const int total = (L - 1) * q.B * T * S;
-    unsigned char *sW = sm;                          // weights of layers 1 .. L-1
-    unsigned char *sStage = sm + net_weight_bytes(L);  // NS halo stages of A_BYTES
+    unsigned char *base = sm + ((1024u - (saddr(sm) & 1023u)) & 1023u);  // 1024-byte aligned
+    unsigned char *sW = base;                          // weights of layers 1 .. L-1
+    unsigned char *sStage = base + net_stage_offset(L);  // NS halo stages of kNetStage bytes
 
     for (int e = tid; e < (L - 1) * C; e += kNetThreads) {
         const int l = 1 + e / C, co = e % C;
@@ -174,19 +186,21 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
                          l < L - 1 ? kNetWHidden : kNetWLast, &wbar);
             }
         }
-        const size_t plane = act_plane_px(q.H, q.W);  // 16-byte pixels per chunk plane
-        const size_t Wp = (size_t)q.W + 2;
-        const unsigned int need = (unsigned int)(kNetGroupWarps * S);
+        const unsigned int need = (unsigned int)S;  // one release per tile of the row
+        const int G = (int)gridDim.x;
+        int ready = 0;  // tiles from this one on whose input rows are known complete
         int k = 0;
         for (;; ++k) {
             const int s = k % NS;
-            int item = (int)blockIdx.x + k * (int)gridDim.x;
+            int item = (int)blockIdx.x + k * G;
             if (item >= total) item = -1;
             Item it{};
             if (item >= 0) {
                 if (lane == 0) trace_at(q, item, 0);
                 it = decode(item, q.B, T, S);
-                if (it.l >= 2 && !net_deps(q, it, T, need, lane)) item = -1;
+                if (ready == 0) ready = net_deps(q, item, G, total, T, S, need, lane);
+                if (ready == 0) item = -1;
+                else --ready;
             }
             if (lane == 0) {
                 if (item >= 0) trace_at(q, item, 1);
@@ -206,14 +220,10 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
                     trace_at(q, item, 2);
                     fence_proxy_async_global();
                     mbar_expect_tx(&full[s], (uint32_t)kNetHaloTx);
-                    // padded rows t TR .. t TR + TR + 1, padded pixels 128 xs .. 128 xs + 129
-                    const uint4 *src = reinterpret_cast<const uint4 *>(q.act[(it.l - 1) & 1]) +
-                                       (size_t)it.b * 4 * plane + (size_t)(it.t * TR) * Wp + (size_t)it.xs * TM;
-                    unsigned char *dst = sStage + (size_t)s * A_BYTES;
-                    for (int c = 0; c < 4; ++c)
-                        for (int r = 0; r < TR + 2; ++r)
-                            bulk_g2s(dst + c * PLANE + r * HW * 16, src + c * plane + (size_t)r * Wp, HW * 16,
-                                     &full[s]);
+                    // padded rows t TR .. t TR + TR + 1 of strip xs: one contiguous run
+                    const unsigned char *src = reinterpret_cast<const unsigned char *>(q.act[(it.l - 1) & 1]) +
+                                               (((size_t)it.b * S + it.xs) * (q.H + 2) + (size_t)it.t * TR) * ROWB;
+                    bulk_g2s(sStage + (size_t)s * kNetStage, src, (uint32_t)kNetHaloTx, &full[s]);
                     trace_at(q, item, 3);
                 }
             }
@@ -267,17 +277,17 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
                     }
                     break;
                 }
-                trace_at(q, item, 5);
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const int l = 1 + item / per_layer;
-                const uint32_t a0 = st0 + (uint32_t)(s * A_BYTES), b0 = w0 + (uint32_t)((l - 1) * kNetWHidden);
+                const uint32_t a0 = st0 + (uint32_t)(s * kNetStage), b0 = w0 + (uint32_t)((l - 1) * kNetWHidden);
                 const uint32_t d0 = tmem + (uint32_t)(bb * TR * C);
                 if (l == L - 1)
-                    issue_tile<16>(d0, a0, b0);
+                    issue_conv_tile<16>(d0, a0, b0);
                 else
-                    issue_tile<32>(d0, a0, b0);
+                    issue_conv_tile<32>(d0, a0, b0);
                 mma_commit(&empty[s]);   // the stage may be refilled once these MMAs are done
                 mma_commit(&tfull[bb]);  // the accumulator is complete once these MMAs are done
+                trace_at(q, item, 5);
                 mbar_arrive(&tfull[bb]);
                 last_k = k;
             }
@@ -292,11 +302,11 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
         for (int k = grp;; k += 2) {
             const int bb = k % kNetBufs;
             const bool got = mbar_wait(&tfull[bb], (uint32_t)((k / kNetBufs) & 1));
-            if (!__all_sync(0xffffffffu, got)) {
+            if (!group_all(got, grp)) {  // a wait ran out: the whole group stops
                 if (lane == 0) atomicExch(q.err, 1);
                 break;
             }
-            const int item = tinfo[bb];
+            const int item = tinfo[bb];  // the same for the whole group
             if (item < 0) break;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const bool tr = (warp % kNetGroupWarps) == 0 && lane == 0;
@@ -310,10 +320,12 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[bb]);
+                if (tr) trace_at(q, item, 7);
                 uint4 v[4];
                 gelu_chunks(r, sbias[it.l], v);
                 store_px(q.act[it.l & 1], it.b, q.H, q.W, y, x, v);
-                net_release(q, 1 + (int)(((size_t)(it.l - 1) * q.B + it.b) * T + it.t), lane);
+                if (tr) trace_at(q, item, 8);
+                net_release(q, 1 + (int)(((size_t)(it.l - 1) * q.B + it.b) * T + it.t), grp, tr);
             } else {
                 uint32_t r0;
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n"
@@ -323,9 +335,11 @@ __global__ void __launch_bounds__(kNetThreads, 1) k_cnn_net(const __grid_constan
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[bb]);
+                if (tr) trace_at(q, item, 7);
                 q.yf[((size_t)it.b * q.H + y) * q.W + x] = (__uint_as_float(r0) + sbias[it.l][0]) * q.out_scale;
+                if (tr) trace_at(q, item, 8);
             }
-            if (tr) trace_at(q, item, 7);
+            if (tr) trace_at(q, item, 9);
         }
     }
 
@@ -364,11 +378,13 @@ int net_stages_that_fit(int L)
 
 // One CTA per SM (the shared memory holds one), no more than there are tiles; a cooperative
 // launch, which the driver refuses rather than run with CTAs that are not all resident.
-cudaError_t net_launch(const NetLaunch &q, cudaStream_t stream, int *grid_out)
+cudaError_t net_launch(const NetLaunch &q_in, cudaStream_t stream, int *grid_out)
 {
+    NetLaunch q = q_in;
+    cudaError_t e;
     const size_t smem = net_smem_bytes(q.L, q.stages);
-    cudaError_t e = cudaFuncSetAttribute(k_cnn_net, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_cnn_net, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return e;
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -378,7 +394,7 @@ cudaError_t net_launch(const NetLaunch &q, cudaStream_t stream, int *grid_out)
     const long long items = (long long)(q.L - 1) * q.B * (q.H / TR) * (q.W / TM);
     const int grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm, items));
     if (grid_out) *grid_out = grid;
-    void *args[] = {const_cast<NetLaunch *>(&q)};
+    void *args[] = {&q};
     return cudaLaunchCooperativeKernel((void *)k_cnn_net, grid, kNetThreads, args, smem, stream);
 }
 

@@ -4,18 +4,18 @@
 // tensor cores: D[128 pixels][32 co] += A[128 pixels][16 ci] B[16 ci][32 co], 18 MMAs per tile
 // (9 taps x 2 halves of the 32 input channels), FP32 accumulation in tensor memory.
 //
-// Activations are bf16 in a padded chunk-planar layout: per image 4 planes (plane c holds channels
-// 8c..8c+7 of every pixel, 16 bytes per pixel), each (H + 2) x (W + 2) pixels with a one-pixel
-// periodic frame (padded pixel (y + 1, x + 1) is image pixel (y, x); frame rows and columns hold
-// the periodic neighbours, written by the producing layer's epilogue).  A CTA owns 128
-// consecutive pixels of TR = 2 image rows; its 4-row, 130-pixel halo is then one contiguous
-// 2080-byte run per (plane, row), copied unchanged into shared memory as 4 chunk planes.  In that
-// layout the A operand of tap (dy, dx) is the same K-major "no swizzle" canonical tile (8-pixel
-// core matrices 128 bytes apart, the two K chunks one plane apart) started at another 16-byte
-// address, so the 9 taps need no data movement.  The weights are staged as [tap][chunk][co][8 ci]
-// bf16.  One thread issues the MMAs and commits them to an mbarrier; the warps then read their 32
-// TMEM lanes (pixels) x 32 columns (output channels), add the bias, apply GELU and store bf16.  The
-// last layer (32 -> 1) is the same MMA with N = 16 (15 zero weight columns) writing channel 0
+// Activations are bf16 in chunk planes (plane c holds channels 8c..8c+7 of a pixel, 16 bytes)
+// and in strips: each 128-pixel strip of the image is stored with its two neighbouring pixels
+// and one periodic frame row above and below, row by row, each row as its 4 chunk planes of 130
+// pixels (act_bytes, store_px).  The producing layer's epilogue writes every halo copy.  A CTA
+// owns 128 consecutive pixels of TR = 2 image rows; its 4-row, 130-pixel halo is then one
+// contiguous run, copied unchanged into shared memory as [row][plane][pixel].  In that layout the
+// A operand of tap (dy, dx) is the same K-major "no swizzle" canonical tile (8-pixel core
+// matrices 128 bytes apart, the two K chunks one plane, 2080 bytes, apart) started at another
+// 16-byte address, so the 9 taps need no data movement.  The weights are staged as
+// [tap][chunk][co][8 ci] bf16.  One thread issues the MMAs and commits them to an mbarrier; the
+// warps then read their 32 TMEM lanes (pixels) x 32 columns (output channels), add the bias,
+// apply GELU and store bf16.  The last layer (32 -> 1) is the same MMA with N = 16 (15 zero weight columns) writing channel 0
 // in FP32 times the output scale.  The first layer (3 -> 32) builds its A operand as an im2col
 // tile in shared memory (K = 3 channels x 9 taps = 27, padded to 32) straight from the three FP32
 // input planes times their input scales: 2 MMAs per tile.
@@ -33,22 +33,26 @@ namespace cnntc {
 constexpr int C = 32;        // hidden channels (input and output of the tensor-core layers)
 constexpr int TM = 128;      // pixels per tile (MMA M)
 constexpr int TR = 2;        // image rows per CTA (one tile each, sharing the halo)
-constexpr int HW = TM + 2;   // halo width
-// one channel-chunk plane of the halo; the 16 bytes of padding put the 4 planes on different
-// banks for the pixel-major fill
-constexpr int PLANE = (TR + 2) * HW * 16 + 16;
-constexpr int A_BYTES = 4 * PLANE;               // 33 344
+constexpr int HW = TM + 2;   // halo width (a strip of 128 pixels and its two neighbours)
+constexpr int PLANEB = HW * 16;                  // 2 080: one chunk plane of one halo row
+constexpr int ROWB = 4 * PLANEB;                 // 8 320: one halo row, its 4 chunk planes
+constexpr int A_BYTES = (TR + 2) * ROWB;         // 33 280: a tile's halo, [row][plane][pixel][16 bytes]
 constexpr int NT = 128;                          // 4 warps = 128 TMEM lanes
+// instruction descriptor: D f32, A/B bf16, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc_bf16(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
+
 // per output width NO (32 hidden channels, or 16 for the 32 -> 1 layer: 1 channel + 15 zero
-// weight columns, the smallest MMA N): weights [tap][chunk][NO][8] bf16
+// weight columns, the smallest MMA N): weights [dx][chunk][2 - dy][NO][8] bf16, so that for one
+// (dx, chunk) the kernel rows of consecutive dy (reversed) are consecutive MMA N rows
 template <int NO>
 struct TcShape {
     static constexpr int B_BYTES = 9 * 4 * NO * 16;
     static constexpr int SMEM_BYTES = A_BYTES + B_BYTES;
     static constexpr int TMEM_COLS = NO * TR <= 32 ? 32 : NO * TR;  // allocation: power of 2 >= 32
-    // D f32, A/B bf16, both K-major, N = NO, M = 128
-    static constexpr uint32_t IDESC =
-        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NO >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+    static constexpr uint32_t IDESC = idesc_bf16(NO);
 };
 constexpr unsigned long long kWaitNs = 2000000000ull;  // an mbarrier wait gives up after 2 s
 
@@ -82,29 +86,37 @@ __device__ __forceinline__ float gelu_f(float z)
 // periodic index in [0, n) of i in [-n, 2n)
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// padded chunk-planar activations: 16-byte pixels per plane, 4 planes per image
-__host__ __device__ __forceinline__ size_t act_plane_px(int H, int W) { return (size_t)(H + 2) * (W + 2); }
-__host__ __device__ __forceinline__ size_t act_bytes(int B, int H, int W) { return (size_t)B * 4 * act_plane_px(H, W) * 16; }
+// Activations in strips: image b, strip xs (128 pixels), padded row py (0 .. H + 1), chunk plane
+// c, strip pixel lp (0 .. 129) -> 16 bytes at ((((b S + xs) (H + 2) + py) 4 + c) 130 + lp), S =
+// W / 128.  Strip pixel lp is image column 128 xs + lp - 1 and padded row py is image row py - 1,
+// both periodic, so a tile's halo (rows py = y0 .. y0 + TR + 1 of one strip) is one contiguous
+// run of A_BYTES.
+__host__ __device__ __forceinline__ size_t act_bytes(int B, int H, int W)
+{
+    return (size_t)B * (W / TM) * (H + 2) * ROWB;
+}
 
-// the 4 chunks of image pixel (y, x) of image b, at its padded position and at every frame
-// position that repeats it (H >= 2, W >= 2)
+// the 4 chunks of image pixel (y, x) of image b, at its place in its strip and at every halo
+// position (the neighbouring strips' edge pixels, the frame rows) that repeats it (H >= 2)
 __device__ __forceinline__ void store_px(__nv_bfloat16 *act, int b, int H, int W, int y, int x, const uint4 (&v)[4])
 {
-    const size_t plane = act_plane_px(H, W), Wp = (size_t)W + 2;
-    uint4 *base = reinterpret_cast<uint4 *>(act) + (size_t)b * 4 * plane;
+    const int S = W / TM, xs = x / TM, lp = x - xs * TM + 1;
     const int py1 = y == 0 ? H + 1 : (y == H - 1 ? 0 : -1);
-    const int px1 = x == 0 ? W + 1 : (x == W - 1 ? 0 : -1);
+    // the left neighbour's pixel 129 repeats lp = 1; the right neighbour's pixel 0 repeats lp = 128
+    const int xs1 = lp == 1 ? (xs + S - 1) % S : (lp == TM ? (xs + 1) % S : -1);
+    const int lp1 = lp == 1 ? TM + 1 : 0;
+    uint4 *img = reinterpret_cast<uint4 *>(act) + (size_t)b * S * (H + 2) * (ROWB / 16);
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
         const int py = i == 0 ? y + 1 : py1;
         if (py < 0) continue;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int px = j == 0 ? x + 1 : px1;
-            if (px < 0) continue;
-            uint4 *d = base + (size_t)py * Wp + px;
+            const int s = j == 0 ? xs : xs1;
+            if (s < 0) continue;
+            uint4 *d = img + ((size_t)s * (H + 2) + py) * (ROWB / 16) + (j == 0 ? lp : lp1);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) d[c * plane] = v[c];
+            for (int c = 0; c < 4; ++c) d[c * HW] = v[c];
         }
     }
 }
@@ -114,10 +126,11 @@ template <int NO>
 __global__ void k_pack_weights(const float *__restrict__ w, int Co, __nv_bfloat16 *__restrict__ wtc)
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 9 * 4 * NO * 8; e += gridDim.x * blockDim.x) {
-        const int t = e / (4 * NO * 8), r = e % (4 * NO * 8);
-        const int ch = r / (NO * 8), r2 = r % (NO * 8), co = r2 / 8, k = r2 % 8;
-        const int ci = ch * 8 + k;
-        wtc[e] = __float2bfloat16_rn(co < Co ? w[((size_t)co * C + ci) * 9 + t] : 0.0f);
+        const int dx = e / (4 * 3 * NO * 8), r = e % (4 * 3 * NO * 8);
+        const int ch = r / (3 * NO * 8), r2 = r % (3 * NO * 8);
+        const int j = r2 / (NO * 8), r3 = r2 % (NO * 8), co = r3 / 8, k = r3 % 8;
+        const int ci = ch * 8 + k, dy = 2 - j;
+        wtc[e] = __float2bfloat16_rn(co < Co ? w[((size_t)co * C + ci) * 9 + dy * 3 + dx] : 0.0f);
     }
 }
 
@@ -198,6 +211,36 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem_d)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_d), "r"(COLS));
 }
 
+// The MMAs of one tile (TR = 2 output rows, accumulators NO columns apart from d0): halo row h
+// feeds output row h - dy for every dy with 0 <= h - dy < TR, and those rows share the A
+// operand, so one MMA per (h, dx, K half) covers them all with N = NO x (number of such dy): the
+// weight rows of consecutive dy (reversed) are consecutive in the packed layout, and so are the
+// accumulators of the output rows.  Halo rows 0 and TR + 1 (one output row each) go first and
+// start their accumulator; rows 1 .. TR then accumulate: 6 (TR + 2) = 24 MMAs instead of 36.
+// A from [row][plane][pixel] at a0 (planes PLANEB, rows ROWB bytes apart), B from the layer's
+// packed weights at b0; descriptors built once (their 14-bit start-address field cannot carry:
+// shared memory < 256 KB).
+template <int NO>
+__device__ __forceinline__ void issue_conv_tile(uint32_t d0, uint32_t a0, uint32_t b0)
+{
+    static_assert(TR == 2, "halo-row order written for two output rows");
+    const uint64_t da = smem_desc(a0, PLANEB, 128), db = smem_desc(b0, 3 * NO * 16, 128);
+    constexpr int order[TR + 2] = {0, TR + 1, 1, 2};
+#pragma unroll
+    for (int i = 0; i < TR + 2; ++i) {
+        const int h = order[i];
+        const int dy_lo = h - (TR - 1) > 0 ? h - (TR - 1) : 0, dy_hi = h < 2 ? h : 2;  // valid dy range
+        const int nj = dy_hi - dy_lo + 1, j0 = 2 - dy_hi, r0 = h - dy_hi;             // first output row
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+            for (int kh = 0; kh < 2; ++kh)
+                mma_bf16(d0 + (uint32_t)(NO * r0), da + (uint64_t)((h * ROWB + 2 * kh * PLANEB + dx * 16) >> 4),
+                         db + (uint64_t)((((dx * 4 + 2 * kh) * 3 + j0) * NO * 16) >> 4), idesc_bf16(NO * nj),
+                         (i >= 2 || dx > 0 || kh > 0) ? 1u : 0u);
+    }
+}
+
 // 32 accumulator columns (already loaded) -> bias, GELU, bf16: the pixel's 4 chunks
 __device__ __forceinline__ void gelu_chunks(const uint32_t (&r)[32], const float *bias, uint4 (&v)[4])
 {
@@ -261,33 +304,16 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16 *__restrict_
     const int x0 = (blockIdx.x % tiles_x) * TM;
     const size_t img = (size_t)blockIdx.y * H * W;
 
-    // halo: padded rows y0 .. y0 + TR + 1, padded pixels x0 .. x0 + 129 of each chunk plane; a warp
-    // copies 32 consecutive 16-byte pixels (512 contiguous bytes)
-    const size_t plane = act_plane_px(H, W);
-    const uint4 *xin = reinterpret_cast<const uint4 *>(x) + (size_t)blockIdx.y * 4 * plane;
-    for (int e = tid; e < 4 * (TR + 2) * HW; e += NT) {
-        const int c = e / ((TR + 2) * HW), r = e - c * ((TR + 2) * HW);
-        const int row = r / HW, xi = r - row * HW;
-        cp16(sA + c * PLANE + r * 16, xin + c * plane + (size_t)(y0 + row) * (W + 2) + x0 + xi);
-    }
+    // halo: padded rows y0 .. y0 + TR + 1 of the strip, one contiguous run
+    const uint4 *xin = reinterpret_cast<const uint4 *>(x) +
+                       (((size_t)blockIdx.y * tiles_x + blockIdx.x % tiles_x) * (H + 2) + y0) * (ROWB / 16);
+    for (int e = tid; e < A_BYTES / 16; e += NT) cp16(sA + e * 16, xin + e);
     for (int e = tid; e < B_BYTES / 16; e += NT) cp16(sB + e * 16, wtc + (size_t)e * 8);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     const uint32_t tmem_d = tc_setup<TMEM_COLS>(&tmem_base, &mbar);
 
     if (tid == 0) {
-        const uint32_t a0 = saddr(sA), b0 = saddr(sB);
-#pragma unroll
-        for (int rr = 0; rr < TR; ++rr) {  // output row y0 + rr accumulates in columns [NO rr, NO rr + NO)
-#pragma unroll
-            for (int t = 0; t < 9; ++t) {
-                const int dy = t / 3, dx = t % 3;  // halo row (relative to rr) and pixel offset of the tap
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                    mma_bf16(tmem_d + (uint32_t)(NO * rr),
-                             smem_desc(a0 + (2 * h) * PLANE + ((rr + dy) * HW + dx) * 16, PLANE, 128),
-                             smem_desc(b0 + (t * 4 + 2 * h) * NO * 16, NO * 16, 128), S::IDESC, (t | h) ? 1u : 0u);
-            }
-        }
+        issue_conv_tile<NO>(tmem_d, saddr(sA), saddr(sB));  // output row y0 + rr in columns [NO rr, NO rr + NO)
         mma_commit(&mbar);
     }
     if (mma_wait(&mbar)) {

@@ -102,20 +102,21 @@ def test_deep_network_runs_one_launch_per_layer():
 
 def test_persistent_launch_trace():
     """The per-tile timestamps of a traced persistent launch: every tile recorded, each tile's
-    eight events (taken, inputs complete, stage free, copies issued, copies landed, MMAs issued,
-    epilogue started, released) in that order, and tracing leaves the values alone."""
+    ten events (taken, inputs complete, stage free, copy issued, copy landed, MMAs issued,
+    epilogue started, accumulator read, stores issued, released) in that order, and tracing
+    leaves the values alone."""
     rng = np.random.default_rng(13)
     net = P().CNN(6, 32, seed=9)
     x = rng.standard_normal((1, 3, 64, 256)).astype(np.float32)
     y0 = net.forward_tc(x)
-    assert net.read_trace().shape == (0, 8)
+    assert net.read_trace().shape == (0, 10)
     net.set_trace(True)
     np.testing.assert_array_equal(net.forward_tc(x), y0)
     tr = net.read_trace().astype(np.int64)
-    assert tr.shape == (5 * 32 * 2, 8)
+    assert tr.shape == (5 * 32 * 2, 10)
     assert (tr > 0).all()
     assert (np.diff(tr, axis=1) >= 0).all()
     # the first layer's tiles start before the last layer's end
-    assert tr[:64, 0].min() < tr[-64:, 7].max()
+    assert tr[:64, 0].min() < tr[-64:, 9].max()
     net.set_trace(False)
     net.close()
