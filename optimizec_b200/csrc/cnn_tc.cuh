@@ -352,6 +352,7 @@ struct FirstIn {
 constexpr int PLANE_F = TR * TM * 16;        // bytes of one chunk plane of the im2col tile
 constexpr int B_FIRST = 4 * C * 16;          // 2 KB of weights
 constexpr int SMEM_FIRST = 4 * PLANE_F + B_FIRST;
+constexpr int NT_FIRST = TR * TM;            // 256: one im2col pixel each; warps 4 rr + q read row rr
 
 // w0[co][ci][3][3] f32 -> [chunk][co][8] bf16
 static __global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wtc)
@@ -362,7 +363,7 @@ static __global__ void k_pack_first(const float *__restrict__ w, __nv_bfloat16 *
     }
 }
 
-static __global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const __nv_bfloat16 *__restrict__ wtc,
+static __global__ void __launch_bounds__(NT_FIRST) k_conv_tc_first(FirstIn in, const __nv_bfloat16 *__restrict__ wtc,
                                                       const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y,
                                                       int H, int W, int *__restrict__ err)
 {
@@ -377,12 +378,11 @@ static __global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const _
     const int y0 = (blockIdx.x / tiles_x) * TR;
     const int x0 = (blockIdx.x % tiles_x) * TM;
     const int b = blockIdx.y;
-    for (int e = tid; e < B_FIRST / 16; e += NT) cp16(sB + e * 16, wtc + (size_t)e * 8);
+    for (int e = tid; e < B_FIRST / 16; e += NT_FIRST) cp16(sB + e * 16, wtc + (size_t)e * 8);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    // im2col: thread handles pixels tid and tid + 128 of the TR x 128 tile
-#pragma unroll
-    for (int q = 0; q < TR; ++q) {
-        const int pi = tid + q * TM;  // = rr * 128 + m
+    // im2col: one pixel of the TR x 128 tile per thread
+    {
+        const int pi = tid;  // = rr * 128 + m
         const int rr = pi / TM, m = pi - rr * TM;
         const int yy = y0 + rr, xx = x0 + m;
         const int xm = wrap(xx - 1, W), xp = wrap(xx + 1, W);
@@ -417,12 +417,10 @@ static __global__ void __launch_bounds__(NT) k_conv_tc_first(FirstIn in, const _
         mma_commit(&mbar);
     }
     if (mma_wait(&mbar)) {
-        const int m = warp * 32 + lane;
-#pragma unroll 1
-        for (int rr = 0; rr < TR; ++rr) {
-            const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(C * rr);
-            epilogue32(taddr, bias, y, b, H, W, y0 + rr, x0 + m);
-        }
+        // warp w: TMEM lanes 32 (w % 4) .. (pixels) of output row w / 4
+        const int qd = warp & 3, rr = warp >> 2;
+        const uint32_t taddr = tmem_d + ((uint32_t)(qd * 32) << 16) + (uint32_t)(C * rr);
+        epilogue32(taddr, bias, y, b, H, W, y0 + rr, x0 + qd * 32 + lane);
     } else if (lane == 0) {
         atomicExch(err, 1);
     }

@@ -384,7 +384,7 @@ struct dns2d_state {
     Tuning tune;         // kernel configuration (from the autotuner's table at creation)
     float2 *force = nullptr, *bk_om2 = nullptr, *bk_fnm1 = nullptr, *bk_work = nullptr;
     float *gate = nullptr;                  // device 0/1 per step (energy gate)
-    double2 *gate_part = nullptr;           // per-block partials of the gate reduction
+    double2 *gate_part = nullptr;           // per-column partials of the gate reduction, [H]
     unsigned int *gate_counter = nullptr;
     unsigned long long *gate_off = nullptr; // device count of gated-off steps
     std::map<int, cudaGraphExec_t> closure_graphs;
@@ -2822,7 +2822,7 @@ int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, const dns2d::cnntc::Fi
     const dim3 grid((W / TM) * (H / TR), B);
     const __nv_bfloat16 *w_last = n->wtc + (size_t)(L - 2) * 9 * 32 * 32;
     const __nv_bfloat16 *w_first = w_last + 9 * 4 * 16 * 8;
-    k_conv_tc_first<<<grid, NT, SMEM_FIRST, st>>>(in, w_first, n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
+    k_conv_tc_first<<<grid, NT_FIRST, SMEM_FIRST, st>>>(in, w_first, n->params + n->woff[0] + (size_t)n->co[0] * n->ci[0] * 9,
                                                   n->act_tc[0], H, W, n->tc_err);
     const int stages = n->tc_mode == 1 ? net_stages_that_fit(L) : 0;
     if (stages >= 2) {
@@ -3187,73 +3187,9 @@ __global__ void k_scale_copy(const float *in, float *out, size_t n, float sc)
         out[i] = in[i] * sc;
 }
 
-// Energy gate: the forcing F changes the energy at the rate P = sum w Re(conj(om/K^2) F); the
-// resolved energy of an unforced step can only fall (dE/dt = -2 nu Z), so the closure is kept
-// for this step only when P <= 2 nu Z, otherwise the step runs as the plain coarse step.
-// Grid kGateBlocks x 256: per-block partials, summed by a fixed tree in the last block to arrive.
-constexpr int kGateBlocks = 64;  // <= the gate's 256 threads per block (one partial each in the last block)
-// scale == 0: the forcing is dropped (gate 0) for a step whose energy input P exceeds the viscous
-// loss 2 nu Z; scale == 1: it is scaled by 2 nu Z / P so that its input equals the loss
-__global__ void k_closure_gate(const float2 *om2, const float2 *force, int N, float visc, int scale, float *gate,
-                               unsigned long long *off, double2 *part, unsigned int *counter)
-{
-    __shared__ double sp[256], sz[256];
-    __shared__ bool last;
-    const int H = N / 2;
-    double P = 0.0, Z = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)N * H; i += (size_t)gridDim.x * blockDim.x) {
-        const int kx = (int)(i / N), iz = (int)(i % N);
-        const int kz = (iz < H) ? iz : iz - N;
-        const double k2 = (double)kx * kx + (double)kz * kz;
-        if (k2 == 0.0) continue;
-        const double w = (kx == 0) ? 1.0 : 2.0;
-        const float2 o = om2[i], f = force[i];
-        P += w * ((double)o.x * f.x + (double)o.y * f.y) / k2;
-        Z += 0.5 * w * ((double)o.x * o.x + (double)o.y * o.y);
-    }
-    sp[threadIdx.x] = P;
-    sz[threadIdx.x] = Z;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            sp[threadIdx.x] += sp[threadIdx.x + o];
-            sz[threadIdx.x] += sz[threadIdx.x + o];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        part[blockIdx.x] = make_double2(sp[0], sz[0]);
-        __threadfence();
-        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    // the last block sums the partials: one per thread, then the same tree (a single thread's
-    // loop over them waited out one L2 round trip after another)
-    double2 q = make_double2(0.0, 0.0);
-    if ((int)threadIdx.x < (int)gridDim.x) q = __ldcg(&part[threadIdx.x]);
-    sp[threadIdx.x] = q.x;
-    sz[threadIdx.x] = q.y;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            sp[threadIdx.x] += sp[threadIdx.x + o];
-            sz[threadIdx.x] += sz[threadIdx.x + o];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const double Ps = sp[0], Zs = sz[0];
-        *counter = 0u;
-        const double loss = 2.0 * (double)visc * Zs;
-        const bool keep = Ps <= loss;  // P > loss >= 0 below: the ratio is in [0, 1)
-        *gate = keep ? 1.0f : (scale ? (float)(loss / Ps) : 0.0f);
-        if (!keep) *off += 1ULL;
-    }
-}
-
-// forcing spectrum of the current state into s->force
-int closure_forcing(dns2d_state *s)
+// forcing spectrum of the current state into s->force; with g.om2 set the forcing's column
+// transform also decides the step's energy gate (GateArgs, dns2d_kernels.cuh)
+int closure_forcing(dns2d_state *s, const GateArgs &g = GateArgs{})
 {
     dns2d_cnn *n = s->cnn;
     const int L = s->L;
@@ -3285,7 +3221,7 @@ int closure_forcing(dns2d_state *s)
         DNS2D_LAUNCHED("closure output");
     }
     s->ks->rows_fwd_scalar(p, forcing_field, s->scratch, s->stream);
-    s->ks->cols_fwd_scalar(p, s->scratch, s->force, s->stream);
+    s->ks->cols_fwd_scalar(p, s->scratch, s->force, g, s->stream);
     DNS2D_LAUNCHED("closure transform");
     return DNS2D_OK;
 }
@@ -3296,16 +3232,23 @@ int closure_forcing(dns2d_state *s)
 static int closure_device_step(dns2d_state *s, int first, int slot)
 {
     s->mm_plane2 = 0;  // the closure's inputs are staged in the physical planes
-    int rc = closure_forcing(s);
+    GateArgs g;
+    const bool gated = s->closure_check == 1 || s->closure_check == 3;
+    if (gated) {
+        g.om2 = s->om2;
+        g.visc = s->visc;
+        g.scale = s->closure_check == 3 ? 1 : 0;
+        g.gate = s->gate;
+        g.off = s->gate_off;
+        g.part = s->gate_part;
+        g.counter = s->gate_counter;
+    }
+    int rc = closure_forcing(s, g);
     if (rc) return rc;
     Pointers p = s->ptrs();
     p.force = s->force;
     p.force_clamp = s->closure_clamp;
-    if (s->closure_check == 1 || s->closure_check == 3) {
-        k_closure_gate<<<kGateBlocks, 256, 0, s->stream>>>(s->om2, s->force, s->N, s->visc, s->closure_check == 3 ? 1 : 0,
-                                                          s->gate, s->gate_off, s->gate_part, s->gate_counter);
-        p.gate = s->gate;
-    }
+    if (gated) p.gate = s->gate;
     s->ks->rows_step(p, s->stream, 1);
     s->ks->cols_step(p, first, slot, s->stream, 1);
     DNS2D_LAUNCHED("closed step");
@@ -3440,7 +3383,7 @@ extern "C" int dns2d_closure_attach(dns2d_state *s, dns2d_cnn *n, const float *s
     }
     if (!s->gate) {
         if (cudaMalloc((void **)&s->gate, 4) != cudaSuccess || cudaMalloc((void **)&s->gate_off, 8) != cudaSuccess ||
-            cudaMalloc((void **)&s->gate_part, kGateBlocks * 16) != cudaSuccess ||
+            cudaMalloc((void **)&s->gate_part, (size_t)s->H * 16) != cudaSuccess ||
             cudaMalloc((void **)&s->gate_counter, 4) != cudaSuccess ||
             cudaMemset(s->gate_counter, 0, 4) != cudaSuccess) {
             cudaGetLastError();

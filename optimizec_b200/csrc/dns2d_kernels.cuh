@@ -1269,23 +1269,106 @@ __global__ void __launch_bounds__(Cfg<N>::NTB) k_rows_fwd_scalar(Pointers p, con
     }
 }
 
+// Energy gate of the closure, folded into the forcing's column transform (GateArgs.om2 set): the
+// forcing F changes the energy at the rate P = sum w Re(conj(om / K^2) F); the resolved energy of
+// an unforced step can only fall (dE/dt = -2 nu Z, Z = sum 0.5 w |om|^2; w = 1 at kx = 0, else 2;
+// the mean mode left out), so the closure is kept for this step only when P <= 2 nu Z.  scale 0:
+// otherwise the step runs as the plain coarse step (gate 0); scale 1: the forcing is scaled by
+// 2 nu Z / P so that its input equals the loss.  Each column adds its modes in FP64, the partials
+// (one per column) are summed by a fixed tree in the last column CTA to arrive, which decides.
+__host__ __device__ constexpr int pow2_ceil(int n)
+{
+    int p = 1;
+    while (p < n) p *= 2;
+    return p;
+}
+
+struct GateArgs {
+    const float2 *om2 = nullptr;       // the state's vorticity modes [kx][kz]; nullptr: no gate
+    float visc = 0.0f;
+    int scale = 0;
+    float *gate = nullptr;              // the factor the step applies to the forcing
+    unsigned long long *off = nullptr;  // steps whose forcing was dropped or scaled
+    double2 *part = nullptr;            // (P, Z) per column, [H]
+    unsigned int *counter = nullptr;    // arrival counter, reset by the last CTA
+};
+
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_fwd_scalar(Pointers p, const float2 *scratch, float2 *out)
+__global__ void __launch_bounds__(Cfg<N>::NTA) k_cols_fwd_scalar(Pointers p, const float2 *scratch, float2 *out,
+                                                                  GateArgs g)
 {
     using C = Cfg<N>;
     constexpr int PS = C::PS;
     constexpr int L = C::L, H = C::H, LP = C::LP, NT = C::NTA;
     extern __shared__ float2 smem[];
+    __shared__ double sp[NT], sz[NT];
+    __shared__ bool last;
     const int kx = blockIdx.x;
     for (int z = threadIdx.x; z < L; z += NT) smem[sidx<PS>(z)] = scratch[widx<L, H>(0, z, kx)];
     __syncthreads();
     fft_run<TwCat<N>, L, LP, false, 1, NT, PS>(smem, p.tw, typename C::Plan{});
     const float sc = 1.0f / (float)L;
+    double P = 0.0, Z = 0.0;
+    const double w = (kx == 0) ? 1.0 : 2.0;
     for (int iz = threadIdx.x; iz < N; iz += NT) {
         const int kz = (iz < H) ? iz : iz - N;
         const int kzi = (kz >= 0) ? kz : kz + L;
         const float2 v = smem[sidx<PS>(kzi)];
-        out[(size_t)kx * N + iz] = (kz == -H) ? make_float2(0.f, 0.f) : make_float2(v.x * sc, v.y * sc);
+        const float2 f = (kz == -H) ? make_float2(0.f, 0.f) : make_float2(v.x * sc, v.y * sc);
+        out[(size_t)kx * N + iz] = f;
+        if (g.om2) {
+            const double k2 = (double)kx * kx + (double)kz * kz;
+            if (k2 != 0.0) {
+                const float2 o = g.om2[(size_t)kx * N + iz];
+                P += w * ((double)o.x * f.x + (double)o.y * f.y) / k2;
+                Z += 0.5 * w * ((double)o.x * o.x + (double)o.y * o.y);
+            }
+        }
+    }
+    if (!g.om2) return;
+    // block sums by a fixed tree (NT need not be a power of two), then the column's partial
+    constexpr int P2 = pow2_ceil(NT);
+    sp[threadIdx.x] = P;
+    sz[threadIdx.x] = Z;
+    __syncthreads();
+    for (int o = P2 / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o && (int)threadIdx.x + o < NT) {
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+            sz[threadIdx.x] += sz[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        g.part[kx] = make_double2(sp[0], sz[0]);
+        __threadfence();
+        last = (atomicAdd(g.counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last CTA: each thread adds the partials of columns threadIdx.x, + NT, ..., then the tree
+    double2 q = make_double2(0.0, 0.0);
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += NT) {
+        const double2 r = __ldcg(&g.part[c]);
+        q.x += r.x;
+        q.y += r.y;
+    }
+    sp[threadIdx.x] = q.x;
+    sz[threadIdx.x] = q.y;
+    __syncthreads();
+    for (int o = P2 / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o && (int)threadIdx.x + o < NT) {
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+            sz[threadIdx.x] += sz[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double Ps = sp[0], Zs = sz[0];
+        *g.counter = 0u;
+        const double loss = 2.0 * (double)g.visc * Zs;
+        const bool keep = Ps <= loss;  // P > loss >= 0 below: the ratio is in [0, 1)
+        *g.gate = keep ? 1.0f : (g.scale ? (float)(loss / Ps) : 0.0f);
+        if (!keep) *g.off += 1ULL;
     }
 }
 

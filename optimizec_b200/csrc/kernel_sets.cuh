@@ -22,7 +22,9 @@ struct KernelSet {
     void (*cols_scalar)(const Pointers &, float2 *, int, cudaStream_t);
     void (*rows_scalar)(const Pointers &, const float2 *, float *, float2 *, cudaStream_t);
     void (*rows_fwd_scalar)(const Pointers &, const float *, float2 *, cudaStream_t);
-    void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, cudaStream_t);
+    // forward column transform of the forcing; with GateArgs.om2 set it also decides the closure's
+    // energy gate for the step
+    void (*cols_fwd_scalar)(const Pointers &, const float2 *, float2 *, const GateArgs &, cudaStream_t);
     // full 2D R2C of the physical u, w planes (dump path; nullptr at the cluster sizes)
     void (*velocity_r2c_full)(const Pointers &, const float *, float2 *, cudaStream_t);
     // min / max partials rows_scalar leaves in its `mm` argument (0: none that cover its output)
@@ -148,9 +150,10 @@ struct Launch {
     {
         k_rows_fwd_scalar<N><<<GB, C::NTB, smB, s>>>(p, f, scratch);
     }
-    static void cols_fwd_scalar(const Pointers &p, const float2 *scratch, float2 *out, cudaStream_t s)
+    static void cols_fwd_scalar(const Pointers &p, const float2 *scratch, float2 *out, const GateArgs &g,
+                                cudaStream_t s)
     {
-        k_cols_fwd_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, out);
+        k_cols_fwd_scalar<N><<<C::H, C::NTA, smA1, s>>>(p, scratch, out, g);
     }
     static void velocity_r2c_full(const Pointers &p, const float *phys, float2 *spec, cudaStream_t s)
     {
