@@ -68,10 +68,11 @@ def parse():
                     help="FP64 oracle steps for cpu_baseline (about 10 s on 16 host cores at N=4096)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--profile", choices=["step", "closure"], default=None,
+    ap.add_argument("--profile", choices=["step", "closure", "network"], default=None,
                     help="short run for an ncu capture, nothing timed or printed as a bench line: 'step' = "
                          "k^4 field (seed 1), NEXTDT, 1 + 3 steps of size --n through the step graphs; "
-                         "'closure' = 3 closed steps at N=256 with a 6 x 32 network")
+                         "'closure' = 3 closed steps at N=256 with a 6 x 32 network; 'network' = the "
+                         "persistent network launch on a 384^2 image with its per-tile trace, summarised")
     ap.add_argument("--windows", type=int, default=0,
                     help="number of timed K-step windows (0: as many as fill about 1 s of device time)")
     ap.add_argument("--workload", choices=["dns4096", "dns16384", "dns29400", "ensemble"], default="dns4096",
@@ -599,10 +600,40 @@ def main_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def network_trace_summary(tr, layers, T, S, G):
+    """Medians of a persistent network launch's per-tile trace ([tiles, 10] ns; tiles in layer
+    order, T tile rows x S strips per layer, CTA c took tiles c, c + G, ...)."""
+    import numpy as np
+    names = ["taken", "inputs", "stage", "copy", "landed", "issued", "epilogue", "tmem", "stores", "released"]
+    tr = tr.astype(np.int64)
+    tr = tr - tr.min()
+    per = T * S
+    out = {"tiles": int(len(tr)), "ctas": int(G), "span_us": round(float(tr[:, 9].max() - tr[:, 0].min()) / 1e3, 2),
+           "layers": []}
+    for j in range(layers - 1):
+        a = tr[j * per:(j + 1) * per]
+        d = np.median(np.diff(a, axis=1), axis=0) / 1e3
+        out["layers"].append({"layer": j + 1, "first_taken_us": round(float(a[:, 0].min()) / 1e3, 2),
+                              "last_released_us": round(float(a[:, 9].max()) / 1e3, 2),
+                              "median_us": {f"{names[i]}->{names[i + 1]}": round(float(d[i]), 3) for i in range(9)}})
+    gaps = [np.diff(tr[np.arange(c, len(tr), G), 0]) for c in range(G)]
+    out["tile_interval_per_cta_us"] = round(float(np.median(np.concatenate(gaps))) / 1e3, 3)
+    return out
+
+
 def main_profile(args):
     """The short runs the ncu summaries under profiles/ were captured from."""
     import numpy as np
     import optimizec_b200 as P
+    if args.profile == "network":
+        net = P.CNN(6, 32, seed=1)
+        x = np.random.default_rng(1).standard_normal((1, 3, 384, 384)).astype(np.float32)
+        net.set_trace(True)
+        for _ in range(5):
+            net.forward_tc(x)
+        print(json.dumps(network_trace_summary(net.read_trace(), 6, 192, 3, net.tc_info()[1])), flush=True)
+        net.close()
+        return
     if args.profile == "closure":
         s = P.Solver(256, 1e5, 4.0, 0.1)
         s.init_k4(1)

@@ -142,3 +142,21 @@ def test_reference_arm_initial_field(tmp_path):
         assert np.array_equal(om, O.k4_spectrum(32, 4.0, 0))
     finally:
         bench.select_workload("dns4096", None)
+
+
+def test_network_trace_summary():
+    """The persistent network launch's trace summary: per-layer spans and per-step medians of a
+    synthetic trace (2 layers of 2 tile rows x 1 strip, 2 CTAs, every step 100 ns apart)."""
+    import numpy as np
+    import bench
+    tiles = 4
+    tr = np.zeros((tiles, 10), dtype=np.uint64)
+    for i in range(tiles):
+        tr[i] = 1000 + 500 * i + 100 * np.arange(10)
+    out = bench.network_trace_summary(tr, 3, 2, 1, 2)
+    assert out["tiles"] == 4 and out["ctas"] == 2
+    assert out["span_us"] == round((1500 + 900) / 1e3, 2)
+    assert [l["layer"] for l in out["layers"]] == [1, 2]
+    assert all(v == 0.1 for v in out["layers"][0]["median_us"].values())
+    assert out["layers"][1]["first_taken_us"] == 1.0 and out["layers"][1]["last_released_us"] == 2.4
+    assert out["tile_interval_per_cta_us"] == 1.0
