@@ -199,7 +199,21 @@ def main(argv=None):
     ap.add_argument("--clamp", type=float, default=1.0, help="forcing limiter alpha (0: off)")
     ap.add_argument("--checks", default=None,
                     help="evaluations as energy_check:alpha pairs, e.g. 1:1,3:1 (default: 1:clamp,1:0,0:0)")
+    ap.add_argument("--timing-only", action="store_true",
+                    help="no data or training: time the DNS, plain and closed runs (energy_check 1, the "
+                         "limiter at --clamp) with an untrained 6 x 32 network; the wall-time ratio does "
+                         "not depend on the weights")
     a = ap.parse_args(argv)
+    if a.timing_only:
+        from . import CNN
+        net = CNN(6, 32, seed=1)
+        r = evaluate(net, np.array([5.0, 1.0, 1.0, 0.01], np.float32), Nf=a.nf, Nc=a.nc, Re=a.re, K0=4.0,
+                     seed=100, fine_steps=a.steps, update=1000, check=1, clamp=a.clamp)
+        print(json.dumps({"wall_dns": r["wall_dns"], "closure_wall": r["closure"]["wall"],
+                          "closure_steps": r["closure"]["steps"], "plain_wall": r["plain"]["wall"],
+                          "speedup_closure_vs_dns": r["wall_dns"] / r["closure"]["wall"]}), flush=True)
+        net.close()
+        return
     runs = ([(int(c), float(al)) for c, al in (x.split(":") for x in a.checks.split(","))] if a.checks
             else [(1, a.clamp), (1, 0.0), (0, 0.0)])
     cfg = dict(Nf=a.nf, Nc=a.nc, Re=a.re, K0=4.0, cfl=0.1)

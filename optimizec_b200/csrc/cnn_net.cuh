@@ -5,9 +5,9 @@
 // layer; CTA c takes tiles c, c + G, c + 2G, ... (G CTAs) in that order.  A tile of layer l >= 2
 // needs the tile rows t - 1, t, t + 1 (periodic) of layer l - 1 in every strip; each finished
 // tile counts once in a per-(layer, image, tile row) counter, and the producer waits (bounded)
-// for the three counters before it loads the halo.  Every dependency of
-// a tile has a smaller number, every CTA takes its tiles in increasing order and every CTA is
-// resident, so the smallest unfinished tile can always proceed and the waits end.  The same waits
+// for the three counters before it loads the halo.  Every dependency of a tile has a smaller
+// number, every CTA takes its tiles in increasing order and every CTA is resident, so the
+// smallest unfinished tile can always proceed and the waits end.  The same waits
 // also cover the reuse of the two activation buffers: layer l writes the buffer layer l - 2
 // wrote, and every tile of layer l - 1 that reads those rows (its own dependencies) has finished
 // before layer l's tile starts.
@@ -66,7 +66,7 @@ __host__ __device__ constexpr size_t net_smem_bytes(int L, int stages)
 }
 
 struct NetLaunch {
-    const __nv_bfloat16 *wtc = nullptr;  // layers 1 .. L-2 [tap][chunk][32][8], then layer L-1 [tap][chunk][16][8]
+    const __nv_bfloat16 *wtc = nullptr;  // layers 1 .. L-2 [dx][chunk][2 - dy][32][8], then layer L-1 with 16
     const float *bias[kNetMaxLayers] = {};  // bias of layer l (l = 1 .. L-1)
     __nv_bfloat16 *act[2] = {nullptr, nullptr};  // strip layout; layer 0 wrote act[0], layer l < L-1 writes act[l & 1]
     float *yf = nullptr;                 // last layer: [B][H][W] f32
