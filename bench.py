@@ -68,11 +68,14 @@ def parse():
                     help="FP64 oracle steps for cpu_baseline (about 10 s on 16 host cores at N=4096)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--profile", choices=["step", "closure", "network"], default=None,
+    ap.add_argument("--profile", choices=["step", "closure", "network", "training", "training-tc"], default=None,
                     help="short run for an ncu capture, nothing timed or printed as a bench line: 'step' = "
                          "k^4 field (seed 1), NEXTDT, 1 + 3 steps of size --n through the step graphs; "
                          "'closure' = 3 closed steps at N=256 with a 6 x 32 network; 'network' = the "
-                         "persistent network launch on a 384^2 image with its per-tile trace, summarised")
+                         "persistent network launch on a 384^2 image with its per-tile trace, summarised; "
+                         "'training' = Adam iterations of the 6 x 32 closure network (batch 4 at 384^2 and "
+                         "batch 32 at 48^2) with FP32 and with tensor-core convolutions, timed; 'training-tc' = "
+                         "3 tensor-core Adam iterations at 384^2, batch 4 (for an ncu launch list)")
     ap.add_argument("--windows", type=int, default=0,
                     help="number of timed K-step windows (0: as many as fill about 1 s of device time)")
     ap.add_argument("--workload", choices=["dns4096", "dns16384", "dns29400", "ensemble"], default="dns4096",
@@ -625,6 +628,38 @@ def main_profile(args):
     """The short runs the ncu summaries under profiles/ were captured from."""
     import numpy as np
     import optimizec_b200 as P
+    if args.profile == "training-tc":
+        rng = np.random.default_rng(2)
+        x = rng.standard_normal((4, 3, 384, 384)).astype(np.float32)
+        t = rng.standard_normal((4, 1, 384, 384)).astype(np.float32)
+        net = P.CNN(6, 32, seed=1)
+        net.set_train_tc(True)
+        net.set_dataset(x, t)
+        net.train(3, 4, 1e-3, seed=1)
+        print("profile run done", flush=True)
+        net.close()
+        return
+    if args.profile == "training":
+        import time
+        rng = np.random.default_rng(2)
+        out = {}
+        for (n, hw, batch) in ((8, 384, 4), (64, 48, 32)):
+            x = rng.standard_normal((n, 3, hw, hw)).astype(np.float32)
+            t = rng.standard_normal((n, 1, hw, hw)).astype(np.float32)
+            for tc in (False, True):
+                net = P.CNN(6, 32, seed=1)
+                net.set_train_tc(tc)
+                net.set_dataset(x, t)
+                net.train(3, batch, 1e-3, seed=1)  # warm-up: buffers, weights
+                iters = 20 if tc else 5
+                t0 = time.perf_counter()
+                losses = net.train(iters, batch, 1e-3, seed=2)
+                ms = (time.perf_counter() - t0) / iters * 1e3
+                out[f"{hw}x{hw}_batch{batch}_{'tensor' if tc else 'fp32'}_ms_per_iter"] = round(ms, 3)
+                out[f"{hw}x{hw}_batch{batch}_{'tensor' if tc else 'fp32'}_last_loss"] = round(float(losses[-1]), 5)
+                net.close()
+        print(json.dumps(out), flush=True)
+        return
     if args.profile == "network":
         net = P.CNN(6, 32, seed=1)
         x = np.random.default_rng(1).standard_normal((1, 3, 384, 384)).astype(np.float32)

@@ -224,6 +224,12 @@ int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t, int B, int
 /* keep a training set of count samples on the device; then Adam on random minibatches */
 int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W);
 int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uint64_t seed, double *losses);
+/* Training convolutions on the tensor cores (off by default; channels <= 32): forward, data and
+ * weight gradients as tcgen05 GEMMs over bf16 im2col expansions with FP32 accumulation (the
+ * weight gradient split over the pixels, partials summed in fixed order in FP64); loss, GELU and
+ * Adam stay FP32.  Applies to dns2d_cnn_forward, dns2d_cnn_loss_grad and dns2d_cnn_train; the
+ * gradients then agree with the FP32 ones to bf16 rounding of the operands. */
+int dns2d_cnn_set_train_tc(dns2d_cnn *n, int on);
 /* The same forward on the BF16 tensor-core path: every layer runs as an implicit GEMM on tcgen05
  * (bf16 inputs, weights and activations, FP32 accumulation, GELU in its tanh form).  Needs channels == 32, layers >= 3 and W % 128 == 0 (DNS2D_ERR_SIZE otherwise). */
 int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, float *y);

@@ -45,12 +45,12 @@ SYMBOLS = [
     "dns2d_cnn_forward_tc", "dns2d_closure_tensor_cores", "dns2d_autotune", "dns2d_set_tuning", "dns2d_batch_autotune", "dns2d_closure_clamp",
     "dns2d_movie_scale", "dns2d_movie_frame", "dns2d_prepare", "dns2d_batch_prepare", "dns2d_batch_set_mode",
     "dns2d_batch_set_waits", "dns2d_batch_set_items", "dns2d_cnn_set_tc_mode", "dns2d_cnn_tc_info",
-    "dns2d_cnn_set_trace", "dns2d_cnn_read_trace",
+    "dns2d_cnn_set_trace", "dns2d_cnn_read_trace", "dns2d_cnn_set_train_tc",
 ]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # translation units of libdns2d.so: the C ABI and one unit per group of compiled grid sizes
-SOURCES = ["dns2d_api.cu", "ensemble.cu", "cnn_net.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
+SOURCES = ["dns2d_api.cu", "ensemble.cu", "cnn_net.cu", "cnn_gemm.cu", "sets_small.cu", "sets_256.cu", "sets_mid.cu", "sets_4096.cu", "sets_cluster.cu", "sets_16384.cu",
            "sets_29400.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr"]
@@ -179,6 +179,7 @@ def lib():
         "dns2d_cnn_set_tc_mode": (C.c_int, [vp, C.c_int]),
         "dns2d_cnn_tc_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "dns2d_cnn_set_trace": (C.c_int, [vp, C.c_int]),
+        "dns2d_cnn_set_train_tc": (C.c_int, [vp, C.c_int]),
         "dns2d_cnn_read_trace": (C.c_int, [vp, C.POINTER(C.c_uint64), C.c_int, C.POINTER(C.c_int)]),
         "dns2d_closure_tensor_cores": (C.c_int, [vp, C.c_int]),
         "dns2d_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
@@ -621,6 +622,11 @@ class CNN:
         """1 (default): layers 1 .. L-1 of the tensor-core path in one persistent launch where their
         weights fit in shared memory; 0: one launch per layer (same values bit for bit)."""
         self._chk(self._L.dns2d_cnn_set_tc_mode(self._n, int(mode)))
+
+    def set_train_tc(self, on: bool):
+        """Training convolutions (forward, data and weight gradients) as tcgen05 GEMMs over bf16
+        operands with FP32 accumulation (off by default)."""
+        self._chk(self._L.dns2d_cnn_set_train_tc(self._n, int(bool(on))))
 
     def set_trace(self, on: bool):
         """Record per-tile timestamps in each persistent launch (off by default)."""

@@ -84,8 +84,9 @@ def generate(Nf=512, Nc=64, Re=1e4, K0=4.0, cfl=0.1, seeds=range(8), steps=4000,
     return np.asarray(X, dtype=np.float32), np.asarray(T, dtype=np.float32)
 
 
-def train(X, T, layers=6, channels=32, iters=2000, batch=32, lr=1e-3, seed=0):
-    """Normalise, train on the GPU; returns (network, scales, losses)."""
+def train(X, T, layers=6, channels=32, iters=2000, batch=32, lr=1e-3, seed=0, tensor_cores=False):
+    """Normalise, train on the GPU (convolutions as tcgen05 GEMMs with tensor_cores); returns
+    (network, scales, losses)."""
     s_om = float(X[:, 0].std())
     s_u = float(np.sqrt(0.5 * (X[:, 1].var() + X[:, 2].var())))
     s_out = float(T.std())
@@ -93,6 +94,7 @@ def train(X, T, layers=6, channels=32, iters=2000, batch=32, lr=1e-3, seed=0):
     Xn = X / scales[None, :3, None, None]
     Tn = T / s_out
     net = CNN(layers, channels, seed=seed)
+    net.set_train_tc(tensor_cores)
     net.set_dataset(Xn, Tn)
     losses = net.train(iters, batch, lr, seed=seed + 1)
     return net, scales, losses
@@ -199,6 +201,8 @@ def main(argv=None):
     ap.add_argument("--clamp", type=float, default=1.0, help="forcing limiter alpha (0: off)")
     ap.add_argument("--checks", default=None,
                     help="evaluations as energy_check:alpha pairs, e.g. 1:1,3:1 (default: 1:clamp,1:0,0:0)")
+    ap.add_argument("--fp32-training", action="store_true",
+                    help="train with the FP32 SIMT convolutions instead of the tensor-core GEMMs")
     ap.add_argument("--timing-only", action="store_true",
                     help="no data or training: time the DNS, plain and closed runs (energy_check 1, the "
                          "limiter at --clamp) with an untrained 6 x 32 network; the wall-time ratio does "
@@ -221,7 +225,7 @@ def main(argv=None):
     X, T = generate(seeds=range(a.seeds), steps=a.steps, every=a.every, warm=a.every, **cfg)
     print(json.dumps({"data": list(X.shape), "generate_s": round(time.time() - t, 1)}), flush=True)
     t = time.time()
-    net, sc, _ = train(X, T, iters=20, batch=a.batch, lr=1e-3)
+    net, sc, _ = train(X, T, iters=20, batch=a.batch, lr=1e-3, tensor_cores=not a.fp32_training)
     per = (time.time() - t) / 20
     iters = max(100, int(a.train_seconds / per))
     t = time.time()

@@ -194,6 +194,37 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity)
     return done != 0;
 }
 
+__device__ __forceinline__ void mbar_init(uint64_t *m, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *m, uint32_t count = 1)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(saddr(m)), "r"(count)
+                 : "memory");
+}
+
+// one arrival that also announces the bytes the stage's bulk copies will deliver
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(saddr(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing on m
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *m)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(saddr(m))
+                 : "memory");
+}
+
+// orders this thread's generic-proxy view of global memory with its async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+
 // bounded wait for phase 0 of the mbarrier; false when the limit ran out
 __device__ __forceinline__ bool mma_wait(uint64_t *mbar)
 {

@@ -17,6 +17,7 @@
 #include "kernel_sets.cuh"
 #include "ensemble.cuh"
 #include "cnn.cuh"
+#include "cnn_gemm.cuh"
 #include "cnn_net.cuh"
 #include "cnn_tc.cuh"
 #include "../../include/dns2d.h"
@@ -2669,6 +2670,9 @@ struct dns2d_cnn {
     unsigned long long *trace = nullptr;
     size_t trace_cap = 0;  // tiles
     int trace_on = 0, trace_tiles = 0;
+    // training convolutions as tcgen05 GEMMs (cnn_gemm.cuh) when train_tc is set
+    dns2d::cnngemm::Work gw;
+    int train_tc = 0;
     long long gen = 0, tc_gen = -1;
     std::string err;
 };
@@ -2737,6 +2741,16 @@ int cnn_forward_dev(dns2d_cnn *n, int B, int H, int W, cudaStream_t st = nullptr
 {
     if (!st) st = n->stream;
     const float *in = n->xin;
+    if (n->train_tc) {  // every layer as a tcgen05 GEMM (bf16 operands, FP32 accumulation)
+        for (int l = 0; l < n->layers; ++l) {
+            const float *w = n->params + n->woff[l], *bias = w + (size_t)n->co[l] * n->ci[l] * 9;
+            CNN_CUDA(dns2d::cnngemm::conv_fwd(in, n->ci[l], w, bias, n->co[l], n->z[l],
+                                              l + 1 < n->layers ? n->a[l] : nullptr, B, H, W, n->gw, st),
+                     "tensor-core forward");
+            in = n->a[l];
+        }
+        return DNS2D_OK;
+    }
     for (int l = 0; l < n->layers; ++l) {
         conv(n, in, n->params + n->woff[l], n->params + n->woff[l] + (size_t)n->co[l] * n->ci[l] * 9, n->z[l], B,
              n->ci[l], n->co[l], H, W, st);
@@ -2789,6 +2803,7 @@ int cnn_tc_reserve(dns2d_cnn *n, int B, int H, int W)
         CNN_CUDA(cudaStreamSynchronize(n->stream), "sync");
         cudaFree(n->net_sync);
     cudaFree(n->trace);
+    dns2d::cnngemm::work_free(n->gw);
         n->net_sync = nullptr;
         CNN_CUDA(cudaMalloc((void **)&n->net_sync, words * 4), "network counters alloc");
         CNN_CUDA(cudaMemset(n->net_sync, 0, words * 4), "network counters clear");
@@ -2875,6 +2890,23 @@ int cnn_forward_tc_dev(dns2d_cnn *n, int B, int H, int W, const dns2d::cnntc::Fi
 int cnn_backward_dev(dns2d_cnn *n, int B, int H, int W)
 {
     float *dz = n->gout, *other = n->gtmp;
+    if (n->train_tc && ((size_t)B * H * W) % dns2d::cnngemm::BK == 0) {
+        // weight and data gradients as tcgen05 GEMMs; GELU' is applied in the data-gradient epilogue
+        for (int l = n->layers - 1; l >= 0; --l) {
+            const float *xin = (l == 0) ? n->xin : n->a[l - 1];
+            float *dw = n->grad + n->woff[l];
+            float *db = dw + (size_t)n->co[l] * n->ci[l] * 9;
+            CNN_CUDA(dns2d::cnngemm::conv_wgrad(xin, n->ci[l], dz, n->co[l], dw, db, B, H, W, n->gw, n->stream),
+                     "tensor-core weight gradient");
+            if (l > 0) {
+                CNN_CUDA(dns2d::cnngemm::conv_dgrad(dz, n->co[l], n->params + n->woff[l], n->ci[l], n->z[l - 1], other,
+                                                    B, H, W, n->gw, n->stream),
+                         "tensor-core data gradient");
+                std::swap(dz, other);
+            }
+        }
+        return DNS2D_OK;
+    }
     for (int l = n->layers - 1; l >= 0; --l) {
         const float *xin = (l == 0) ? n->xin : n->a[l - 1];
         float *dw = n->grad + n->woff[l];
@@ -3055,6 +3087,26 @@ extern "C" int dns2d_cnn_read_trace(dns2d_cnn *n, unsigned long long *out, int c
     return DNS2D_OK;
 }
 
+extern "C" int dns2d_cnn_set_train_tc(dns2d_cnn *n, int on)
+{
+    if (!n || on < 0 || on > 1) return DNS2D_ERR_ARG;
+    if (on && n->channels > dns2d::cnngemm::BN)
+        return nfail(n, DNS2D_ERR_SIZE, "tensor-core training needs at most 32 channels");
+    n->train_tc = on;
+    return DNS2D_OK;
+}
+
+// the tensor-core training GEMMs' wait flag (0 when no GEMM ran); the stream is synchronised
+static int train_tc_status(dns2d_cnn *n)
+{
+    if (!n->gw.err) return DNS2D_OK;
+    int flag = 0;
+    CNN_CUDA(cudaMemcpyAsync(&flag, n->gw.err, 4, cudaMemcpyDeviceToHost, n->stream), "flag copy");
+    CNN_CUDA(cudaStreamSynchronize(n->stream), "flag sync");
+    if (flag) return nfail(n, DNS2D_ERR_TIMEOUT, "tensor-core training GEMM wait timed out");
+    return DNS2D_OK;
+}
+
 extern "C" int dns2d_cnn_tc_info(const dns2d_cnn *n, int *mode, int *grid)
 {
     if (!n) return DNS2D_ERR_ARG;
@@ -3101,7 +3153,7 @@ extern "C" int dns2d_cnn_loss_grad(dns2d_cnn *n, const float *x, const float *t,
         return rc;
     if (grad) CNN_CUDA(cudaMemcpyAsync(grad, n->grad, (size_t)n->nparams * 4, cudaMemcpyDeviceToHost, n->stream), "grad copy");
     CNN_CUDA(cudaStreamSynchronize(n->stream), "grad sync");
-    return DNS2D_OK;
+    return train_tc_status(n);
 }
 
 extern "C" int dns2d_cnn_set_dataset(dns2d_cnn *n, const float *x, const float *t, int count, int H, int W)
@@ -3160,7 +3212,7 @@ extern "C" int dns2d_cnn_train(dns2d_cnn *n, int iters, int batch, float lr, uin
     }
     CNN_CUDA(cudaStreamSynchronize(n->stream), "train sync");
     n->gen += 1;
-    return DNS2D_OK;
+    return train_tc_status(n);
 }
 
 // ============================================================================================
