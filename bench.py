@@ -408,8 +408,8 @@ def main_ours(args):
                    "timing": "value = K / median device time of consecutive K-step windows (CUDA events on "
                              "the solver's stream), each window ending on a diagnostic step"},
         "mpts_steps_per_s": round(r["value"] * N * N / 1e6, 1),
-        "step_roofline": {"bytes_per_step_survey": 76 * N * N, "bytes_per_step_min": 64 * N * N,
-                          "frac_survey": round(76 * N * N * steps_s / (peak * 1e9), 4),
+        "step_roofline": {"bytes_per_step_model": 76 * N * N, "bytes_per_step_min": 64 * N * N,
+                          "frac_model": round(76 * N * N * steps_s / (peak * 1e9), 4),
                           "frac_min": round(64 * N * N * steps_s / (peak * 1e9), 4)},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),

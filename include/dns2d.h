@@ -50,7 +50,7 @@ int dns2d_create(dns2d_state **out, int N, float Re, float K0, float cflnum, int
 void dns2d_destroy(dns2d_state *s);
 const char *dns2d_strerror(int code);
 const char *dns2d_last_error(const dns2d_state *s);
-/* 1 when N is supported by this build, else 0 */
+/* 1 when N has compiled kernels in this library, else 0 */
 int dns2d_supported(int N);
 /* device bytes held by a state of size N */
 size_t dns2d_device_bytes(int N);
