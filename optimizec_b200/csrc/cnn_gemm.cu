@@ -51,6 +51,24 @@ __global__ void k_im2col_rows(const float *__restrict__ x, int C, int H, int W, 
         const float *xb = x + (size_t)b * C * HW;
         __nv_bfloat16 *Am = A + (size_t)(m / BM) * KS * A_BLOCK;
         const int r = m % BM;
+        if ((C & 7) == 0) {
+            // C a multiple of 8: each 8-k chunk is 8 channels of one tap, one source offset per tap
+            int k8 = 0;
+            for (int tap = 0; tap < 9; ++tap) {
+                const int sy = (y + tap / 3 - 1 + H) % H, sx = (xx + tap % 3 - 1 + W) % W;
+                const float *src = xb + (size_t)sy * W + sx;
+                for (int c0 = 0; c0 < C; c0 += 8, ++k8) {
+                    float v[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) v[i] = valid ? __ldg(src + (size_t)(c0 + i) * HW) : 0.0f;
+                    *reinterpret_cast<uint4 *>(Am + (size_t)(k8 >> 1) * A_BLOCK + a_elem(r, (k8 & 1) * 8)) = pack8(v);
+                }
+            }
+            const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+            for (; k8 < KS * 2; ++k8)
+                *reinterpret_cast<uint4 *>(Am + (size_t)(k8 >> 1) * A_BLOCK + a_elem(r, (k8 & 1) * 8)) = z;
+            continue;
+        }
         int tap = 0, c = 0, off = 0;
         bool newtap = true;
         for (int k8 = 0; k8 < KS * 2; ++k8) {
