@@ -124,6 +124,42 @@ __global__ void k_im2col_cols(const float *__restrict__ x, int C, int H, int W, 
                     pack8(m == 9 * C ? one : zero);
             continue;
         }
+        const int dx = tap % 3;
+        {
+            // W a multiple of 8: the 8 pixels are one row segment x0 .. x0 + 7 (x0 a multiple of
+            // 8); away from the periodic wrap their taps are one aligned 12-float window read as
+            // float4s: dx = 0 needs x0 - 1 .. x0 + 6, dx = 1 x0 .. x0 + 7, dx = 2 x0 + 1 .. x0 + 8
+            const int k0 = k8 * 8, b = k0 / HW, p = k0 - b * HW, y = p / W, x0 = p - y * W;
+            if ((W & 7) == 0 && !(dx == 0 && x0 == 0) && !(dx == 2 && x0 + 8 == W)) {
+                const int sy = (y + tap / 3 - 1 + H) % H;
+                const float *row = x + (size_t)b * C * HW + (size_t)sy * W;
+                for (int c = 0; c < C; ++c) {
+                    const float *rp = row + (size_t)c * HW;
+                    float v[8];
+                    if (dx == 1) {
+                        const float4 a = __ldg(reinterpret_cast<const float4 *>(rp + x0));
+                        const float4 d = __ldg(reinterpret_cast<const float4 *>(rp + x0 + 4));
+                        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+                        v[4] = d.x; v[5] = d.y; v[6] = d.z; v[7] = d.w;
+                    } else {
+                        const int w0 = dx == 0 ? x0 - 4 : x0;
+                        const float4 a = __ldg(reinterpret_cast<const float4 *>(rp + w0));
+                        const float4 d = __ldg(reinterpret_cast<const float4 *>(rp + w0 + 4));
+                        const float4 f = __ldg(reinterpret_cast<const float4 *>(rp + w0 + 8));
+                        if (dx == 0) {
+                            v[0] = a.w; v[1] = d.x; v[2] = d.y; v[3] = d.z;
+                            v[4] = d.w; v[5] = f.x; v[6] = f.y; v[7] = f.z;
+                        } else {
+                            v[0] = a.y; v[1] = a.z; v[2] = a.w; v[3] = d.x;
+                            v[4] = d.y; v[5] = d.z; v[6] = d.w; v[7] = f.x;
+                        }
+                    }
+                    const int m = tap * C + c;
+                    *reinterpret_cast<uint4 *>(Ak + (size_t)(m / BM) * A_BLOCK + a_elem(m % BM, kk)) = pack8(v);
+                }
+                continue;
+            }
+        }
         size_t src[8];
         {
             const int k0 = k8 * 8;
