@@ -634,6 +634,7 @@ cudaError_t conv_fwd(const float *x, int Ci, const float *w, const float *bias, 
 {
     if (Ci < 1 || Ci > BN || Co < 1 || Co > BN) return cudaErrorInvalidValue;
     const int M = B * H * W, MT = (M + BM - 1) / BM, KS = ksteps_of(Ci);
+    if (KS > MAX_KS) return cudaErrorInvalidValue;  // the shared-memory stages are sized for it
     cudaError_t e = ensure(wk, (size_t)MT * KS * A_BLOCK, (size_t)KS * B_BLOCK, 0, st);
     if (e != cudaSuccess) return e;
     k_im2col_rows<<<blocks_for((long long)MT * BM), 256, 0, st>>>(x, Ci, H, W, M, MT, KS, wk.A);
@@ -656,6 +657,7 @@ cudaError_t conv_dgrad(const float *dz, int Co, const float *w, int Ci, const fl
 {
     if (Ci < 1 || Ci > BN || Co < 1 || Co > BN) return cudaErrorInvalidValue;
     const int M = B * H * W, MT = (M + BM - 1) / BM, KS = ksteps_of(Co);
+    if (KS > MAX_KS) return cudaErrorInvalidValue;
     cudaError_t e = ensure(wk, (size_t)MT * KS * A_BLOCK, (size_t)KS * B_BLOCK, 0, st);
     if (e != cudaSuccess) return e;
     k_im2col_rows<<<blocks_for((long long)MT * BM), 256, 0, st>>>(dz, Co, H, W, M, MT, KS, wk.A);
@@ -678,6 +680,7 @@ cudaError_t conv_wgrad(const float *x, int Ci, const float *dz, int Co, float *d
     const int K = B * H * W, HW = H * W;
     if (Ci < 1 || Ci > BN || Co < 1 || Co > BN || K % BK != 0) return cudaErrorInvalidValue;
     const int MT = 9 * Ci / BM + 1, KS = K / BK, nchunks = (KS + KC - 1) / KC;  // rows 0 .. 9 Ci
+    if (MT > MAX_MT) return cudaErrorInvalidValue;  // the shared-memory stages are sized for it
     const int G = std::min(nchunks, sm_count());
     cudaError_t e = ensure(wk, (size_t)KS * MT * A_BLOCK, (size_t)KS * B_BLOCK, (size_t)G * MT * BM * BN, st);
     if (e != cudaSuccess) return e;
