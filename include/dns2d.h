@@ -238,7 +238,9 @@ int dns2d_cnn_forward_tc(dns2d_cnn *n, const float *x, int B, int H, int W, floa
  * three input tile rows of the previous layer) wherever the weights of those layers fit in shared
  * memory (layers <= 8), else one launch per layer; mode 0 always one launch per layer.  Both give
  * the same values bit for bit.  tc_info reports the mode and the grid of the last persistent
- * launch (0 before any). */
+ * launch (0 before any).  The mode (and the trace below) applies to launches made after the
+ * call; a state's already captured closed-step graphs keep theirs until the closure is attached
+ * again. */
 int dns2d_cnn_set_tc_mode(dns2d_cnn *n, int mode);
 int dns2d_cnn_tc_info(const dns2d_cnn *n, int *mode, int *grid);
 /* Per-tile timestamps of the persistent launch (globaltimer ns; off by default): with tracing on,
